@@ -1,0 +1,179 @@
+"""
+Generate the golden fixtures under ``tests/golden/`` by running the REFERENCE MacroMax package (NumPy backend).
+
+Run from the repository root, where the reference tree is present:
+
+    python tests/golden/make_golden.py
+
+Every case builds a reference ``macromax.Solution`` on seeded synthetic inputs (``macromax_b200.workloads``) and
+records the preconditioner constants (alpha, beta), the field E after selected iterations, the residue and
+update-norm history, the iteration count at which the workload's stopping rule fires, and the converged field.
+Inputs are stored in the fixture too, so the fixtures do not depend on the generators staying bit-identical.
+The fixtures pin both the numpy oracle (``oracle/mmoracle.py``) and, through it and directly, the CUDA path.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from refimport import import_reference  # noqa: E402
+from macromax_b200 import workloads  # noqa: E402
+
+RECORD = (1, 2, 3, 5, 10, 20)
+
+
+def run_reference(mm, wl, dtype, record=RECORD, rtol=None, maxiter=None, source=None, store_dtype=None):
+    from macromax.bound import Bound
+    from macromax.utils.ft import Grid
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    bound = Bound(grid, thickness=wl['bound_thickness'])
+    src = wl['source'] if source is None else source
+    sol = mm.Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'], source_distribution=src,
+                      bound=bound, dtype=dtype)
+    alpha0 = complex(sol._Solution__alpha)
+    beta = float(sol._Solution__beta)
+    rtol = wl['rtol'] if rtol is None else rtol
+    maxiter = wl['maxiter'] if maxiter is None else maxiter
+    fields, residues, update_norms, alphas = {}, [], [], []
+    t0 = time.perf_counter()
+    for s in sol:
+        residues.append(s.residue)
+        update_norms.append(s.previous_update_norm)
+        alphas.append(complex(s._Solution__alpha))
+        if s.iteration in record:
+            fields[s.iteration] = s.E.copy()
+        if not (s.iteration < maxiter and s.residue > rtol):
+            break
+    elapsed = time.perf_counter() - t0
+    sd = store_dtype or dtype
+    out = dict(alpha0=np.complex128(alpha0), beta=np.float64(beta), iterations=np.int64(sol.iteration),
+               residues=np.asarray(residues), update_norms=np.asarray(update_norms), alphas=np.asarray(alphas),
+               final=sol.E.astype(sd), rtol=np.float64(rtol), maxiter=np.int64(maxiter),
+               record=np.asarray(sorted(fields)), seconds=np.float64(elapsed))
+    for it, f in fields.items():
+        out[f'E_{it}'] = f.astype(sd)
+    return out
+
+
+def save_case(name, wl, result, store_inputs=True, input_dtype=np.complex128):
+    payload = dict(result)
+    payload['shape'] = np.asarray(wl['shape'])
+    payload['step'] = np.float64(wl['step'])
+    payload['wavelength'] = np.float64(wl['wavelength'])
+    payload['bound_thickness'] = np.float64(wl['bound_thickness'])
+    if store_inputs:
+        payload['epsilon'] = np.asarray(wl['epsilon'], dtype=input_dtype)
+        payload['source'] = np.asarray(wl['source'], dtype=input_dtype)
+    path = os.path.join(HERE, f'{name}.npz')
+    np.savez_compressed(path, **payload)
+    print(f'{name}: iterations={int(result["iterations"])} alpha={complex(result["alpha0"]):.10g} '
+          f'residue={result["residues"][-1]:.3e} ({float(result["seconds"]):.1f}s) -> {os.path.getsize(path)} B')
+
+
+def plane_wave_1d(vectorial: bool, anisotropic: bool = False):
+    """The 1D plane-wave problem of the reference's test_solution.py:91-358, as source_distribution."""
+    import scipy.constants as const
+    wavelength = 500e-9
+    k0 = 2 * np.pi / wavelength
+    nb = 1024
+    pitch = wavelength / 16
+    bt = 10e-6
+    x = pitch * np.arange(nb) - bt
+    frac = np.maximum((x[0] + bt) - x, x - (x[-1] - bt)) / bt
+    frac = np.maximum(0, frac)
+    n = 1 + 1j * 0.1 * frac
+    eps = n ** 2
+    if anisotropic:
+        eps = eps * np.eye(3)[..., None]
+        eps[:, :, frac <= 0] = np.array([[1.1, 0.0, 0.3], [0.0, 1.0, 0.0], [0.3, 0.0, 1.1]])[..., None]
+    j = np.zeros(x.shape)
+    j[np.argmin(np.abs(x))] = 1.0
+    if vectorial:
+        j = np.array([0, 1, 0])[:, None] * j[None, :]
+    else:
+        j = j[None, :]
+    j = j.astype(np.complex64)
+    omega = k0 * const.c
+    src = j * (-1j * omega * const.mu_0)
+    return dict(shape=(nb,), step=pitch, wavelength=wavelength, epsilon=eps, source=src.astype(np.complex64),
+                bound_thickness=0.0, rtol=1e-6, maxiter=10000)
+
+
+def gain_case():
+    """A 2D scalar medium with a small gain inclusion: the divergence guard rejects updates and bumps alpha."""
+    rng = np.random.default_rng(7)
+    wl = workloads.disks_2d(n=48, seed=7)
+    eps = wl['epsilon'].copy()
+    eps[20:28, 20:28] = 2.0 - 0.4j
+    eps += 0.02j * rng.uniform(size=eps.shape)
+    wl['epsilon'] = eps
+    wl['rtol'] = 1e-5
+    wl['maxiter'] = 200
+    return wl
+
+
+def backend_ops(mm):
+    """Known outputs of the reference NumPy backend's per-op methods on seeded random inputs."""
+    from macromax.backend.numpy import BackEndNumpy
+    from macromax.utils.ft import Grid
+    rng = np.random.default_rng(11)
+    grid = Grid([5, 10, 20], 100e-9)
+    k0 = 10e6
+    be = BackEndNumpy(3, grid * k0, hardware_dtype=np.complex128)
+    x = (rng.standard_normal((3, 1, 5, 10, 20)) + 1j * rng.standard_normal((3, 1, 5, 10, 20)))
+    out = dict(x=x)
+    out['ft'] = be.ft(x.copy()).copy()
+    out['ift'] = be.ift(x.copy()).copy()
+    out['longitudinal'] = be.longitudinal_projection_ft(x.copy()).copy()
+    out['transversal'] = be.transversal_projection_ft(x.copy()).copy()
+    out['curl_ft'] = be.curl_ft(x.copy()).copy()
+    out['k2'] = np.asarray(be.k2).copy()
+    for i in range(3):
+        out[f'k{i}'] = np.asarray(be.k[i]).copy()
+    chi = rng.standard_normal((3, 3, 5, 10, 20)) + 1j * rng.standard_normal((3, 3, 5, 10, 20))
+    out['chi'] = chi
+    out['mul'] = be.mul(chi, x.copy()).copy()
+    out['norm'] = np.float64(be.norm(x))
+    path = os.path.join(HERE, 'backend_ops.npz')
+    np.savez_compressed(path, **out)
+    print(f'backend_ops -> {os.path.getsize(path)} B')
+
+
+def main():
+    mm = import_reference()
+    backend_ops(mm)
+
+    wl = workloads.disks_2d(n=64, seed=1)
+    save_case('disks2d_64_c128', wl, run_reference(mm, wl, np.complex128))
+    rec3 = (1, 2, 5, 20)
+    wl = workloads.spheres_3d(n=20, seed=2, nb_spheres=30, boundary_px=32)  # 5-voxel ramp
+    save_case('spheres3d_20_c128', wl, run_reference(mm, wl, np.complex128, record=rec3, maxiter=600))
+    wl = workloads.voronoi_3d(n=16, seed=3, nb_grains=8, boundary_px=48)  # 4-voxel ramp
+    save_case('voronoi3d_16_c128', wl, run_reference(mm, wl, np.complex128, record=rec3, rtol=1e-8, maxiter=600))
+    wl = workloads.design_3d(n=24, seed=5)
+    save_case('design3d_24_c128', wl, run_reference(mm, wl, np.complex128, record=rec3))
+    wl = gain_case()
+    save_case('gain2d_48_c128', wl, run_reference(mm, wl, np.complex128))
+    for vec, aniso, name in ((False, False, 'plane1d_scalar_c64'), (True, False, 'plane1d_vector_c64'),
+                             (True, True, 'plane1d_aniso_c64')):
+        wl = plane_wave_1d(vec, aniso)
+        save_case(name, wl, run_reference(mm, wl, np.complex64, record=(1, 2, 5, 20)), input_dtype=np.complex128)
+    # full-size 256^2 disks (the complex128 configuration): inputs come from the seeded generator (checksummed)
+    wl = workloads.disks_2d(n=256, seed=1)
+    res = run_reference(mm, wl, np.complex128, record=(1, 20), store_dtype=np.complex64)
+    res['epsilon_checksum'] = np.float64(np.sum(np.abs(wl['epsilon']) * np.arange(wl['epsilon'].size).reshape(
+        wl['epsilon'].shape) % 1009))
+    res['source_checksum'] = np.float64(np.sum(np.abs(wl['source'])))
+    save_case('disks2d_256_c128', wl, res, store_inputs=False)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,65 @@
+"""
+Import the reference ``macromax`` package for fixture generation (and for the optional CPU-side integration test).
+
+The reference package writes a log file next to itself on import (``macromax/__init__.py:61-67``) and needs
+``coloredlogs`` and installed package metadata, neither of which exists here.  So this helper copies the package to
+a temporary directory, puts a minimal ``coloredlogs`` stand-in on ``sys.path`` and answers the version lookup.
+It reads the reference tree, so it is only usable where that tree exists; nothing that runs on a GPU box uses it.
+"""
+from __future__ import annotations
+
+import importlib
+import importlib.metadata
+import os
+import shutil
+import sys
+import tempfile
+
+REFERENCE_PYTHON = os.environ.get('MACROMAX_REFERENCE', '/root/reference/python')
+
+_STUB = '''
+import logging
+DEFAULT_FIELD_STYLES = {'asctime': {}}
+DEFAULT_LEVEL_STYLES = {}
+def enable_ansi_support():
+    pass
+class ColoredFormatter(logging.Formatter):
+    def __init__(self, fmt=None, datefmt=None, field_styles=None, level_styles=None):
+        super().__init__(fmt)
+'''
+
+
+def reference_available() -> bool:
+    return os.path.isdir(os.path.join(REFERENCE_PYTHON, 'macromax'))
+
+
+def import_reference():
+    """Return the reference ``macromax`` module, imported from a private copy."""
+    if 'macromax' in sys.modules and getattr(sys.modules['macromax'], '_graft_reference_copy', False):
+        return sys.modules['macromax']
+    if not reference_available():
+        raise ImportError(f'reference package not found under {REFERENCE_PYTHON}')
+    tmp = tempfile.mkdtemp(prefix='macromax_ref_')
+    shutil.copytree(os.path.join(REFERENCE_PYTHON, 'macromax'), os.path.join(tmp, 'macromax'))
+    stubs = os.path.join(tmp, '_stubs')
+    os.makedirs(stubs)
+    with open(os.path.join(stubs, 'coloredlogs.py'), 'w') as f:
+        f.write(_STUB)
+    sys.path.insert(0, stubs)
+    sys.path.insert(0, tmp)
+    original_version = importlib.metadata.version
+
+    def version(name):
+        if name == 'macromax':
+            return '0+reference'
+        return original_version(name)
+
+    importlib.metadata.version = version
+    mm = importlib.import_module('macromax')
+    mm._graft_reference_copy = True
+    import logging
+    mm.log.setLevel(logging.ERROR)
+    for h in list(mm.log.handlers):
+        if isinstance(h, logging.FileHandler):
+            mm.log.removeHandler(h)
+    return mm
