@@ -1,0 +1,317 @@
+"""
+Benchmark of the B200 split-Richardson iteration (voxel-iterations per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload spheres3d] [--n 128]
+
+Workload (default): 3D vector Maxwell, isotropic, complex64, 128^3 grid, 200 seeded spheres, 12-voxel absorbing
+ramp, x-polarised Gaussian sheet source (macromax_b200.workloads.spheres_3d).  A step is one iteration
+d = chi [G (chi E + s') - E] with the divergence guard and update, on inputs resident in HBM; the working set
+(two field buffers, work buffer, source and chi: 208 MB) is larger than the 126 MB L2, so nothing is flushed
+between steps.  ``e2e`` is one full solve to the workload's residue through the public API from host numpy arrays
+(host->device copies of chi, source and initial field and the device->host copy of the solution inside the timed
+region).  ``--impl reference`` times the numpy oracle (the reference NumPy backend's algorithm) on the host cores.
+Multi-GPU: the path does not shard a single grid, so N > 1 runs N independent replicas (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'voxel-iterations/s (split-Richardson iteration)'
+UNIT = 'voxel-it/s'
+
+
+def word_bytes(dtype) -> int:
+    return 16 if np.dtype(dtype) == np.complex128 else 8
+
+
+def algorithmic_bytes(nvox: int, c: int, m: int, dtype, batch: int = 1) -> float:
+    """Compulsory traffic of one iteration: sizeof(word) (8c + 2m/B) per voxel-RHS."""
+    return word_bytes(dtype) * (8 * c + 2 * m / batch) * nvox * batch
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        try:
+            proc = subprocess.Popen(['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.QUERY}',
+                                     '--format=csv,noheader,nounits', '-lms', '200'],
+                                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return
+        try:
+            while not self._stop.is_set():
+                line = proc.stdout.readline()
+                if not line:
+                    break
+                self.samples.append([x.strip() for x in line.split(',')])
+        finally:
+            proc.terminate()
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._thread.join(timeout=3)
+
+    def summary(self):
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace('.', '').isdigit()]
+        smax = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = set()
+        for s in self.samples:
+            for i, nme in enumerate(names):
+                if len(s) > 5 + i and s[5 + i].lower().startswith('active'):
+                    reasons.add(nme)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': max(smax) if smax else None,
+                'reasons': sorted(reasons), 'samples': len(self.samples)}
+
+
+def make_workload(args):
+    from macromax_b200 import workloads
+    if args.workload == 'spheres3d':
+        return workloads.spheres_3d(n=args.n)
+    if args.workload == 'disks2d':
+        return workloads.disks_2d(n=args.n)
+    if args.workload == 'design3d':
+        return workloads.design_3d(n=args.n)
+    if args.workload == 'voronoi3d':
+        return workloads.voronoi_3d(n=args.n)
+    raise SystemExit(f'unknown workload {args.workload}')
+
+
+def dist_setup(args):
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = 'nccl' if args.impl == 'ours' else 'gloo'
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def cpu_oracle_rate(wl, dtype, iters: int, workers: int):
+    """Oracle (reference algorithm, numpy/pocketfft) voxel-iterations/s on the host, over ``iters`` iterations."""
+    from oracle import mmoracle as mo
+    mo.set_fft_workers(workers)
+    sol = mo.from_workload(wl, dtype)
+    sol.advance()  # warm-up iteration
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        sol.advance()
+    dt = time.perf_counter() - t0
+    return int(np.prod(wl['shape'])) * iters / dt, dt
+
+
+def bench_reference(args, wl, rank, world, pg):
+    """--impl reference: the oracle's iteration on the host cores, one iteration per step."""
+    dtype = np.complex64
+    cores = os.cpu_count() or 1
+    if rank != 0:
+        return
+    from oracle import mmoracle as mo
+    mo.set_fft_workers(cores)
+    sol = mo.from_workload(wl, dtype)
+    for _ in range(args.warmup):
+        sol.advance()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sol.advance()
+    dt = time.perf_counter() - t0
+    nvox = int(np.prod(wl['shape']))
+    value = nvox * args.steps / dt
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': args.gpus,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * dt / args.steps, 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic (seeded generator)',
+        'config': config_of(args, wl),
+        'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+                         'sample': f'{args.steps} iterations of the numpy oracle on the full workload, '
+                                   f'scipy.fft pocketfft with {cores} workers'},
+        'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, wl):
+    c = 3 if np.asarray(wl['source']).ndim > len(wl['shape']) and np.asarray(wl['source']).shape[0] == 3 else 1
+    return {'workload': f"{wl['name']}: {'x'.join(map(str, wl['shape']))} grid, {c}-component field, "
+                        f"isotropic chi, complex64, 1 RHS", 'grid': list(wl['shape']), 'components': c,
+            'batch': 1, 'l2': 'working set > L2 (no flush needed)'}
+
+
+def bench_ours(args, wl, rank, world, local, pg):
+    import torch
+    from macromax_b200 import Bound, Grid, Solution
+    from macromax_b200 import _native as nat
+    torch.cuda.set_device(local)
+    dtype = np.complex64
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    bound = Bound(grid, thickness=wl['bound_thickness'])
+    sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                   source_distribution=wl['source'], bound=bound, dtype=dtype)
+    eng = sol._engine
+    nvox = eng.N
+    c = eng.ncomp
+    m = 1 if eng.chi_kind == nat.MMX_CHI_SCALAR else 9
+    # keep every step a real iteration: disable the stop rule
+    st = eng.read_state()
+    st['rtol'] = -1.0
+    st['maxiter'] = np.inf
+    st['active'] = 1
+    eng.write_state(st)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        eng.iterate(1)
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        eng.iterate(args.steps)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    ms = start.elapsed_time(stop)
+    if pg is not None:
+        t = torch.tensor([ms], device='cuda')
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * nvox * args.steps / (ms / 1e3)
+    st = eng.read_state()
+    assert np.all(st['status'] == 0) and np.all(st['iteration'] >= args.steps), 'iteration did not run'
+    launches_per_iter = len_passes(wl) + 1
+    # roofline over one iteration
+    alg = algorithmic_bytes(nvox, c, m, dtype)
+    peaks = load_peaks()
+    achieved = alg / (ms_per_step / 1e3) / 1e9
+    roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+            'frac': achieved / peaks['hbm_gbs'], 'traffic': None, 'peak_source': peaks['source'],
+            'unit_of_launch': 'one iteration (pass kernels + decide)', 'algorithmic_bytes': alg}
+    # end to end: one full solve through the public API from host arrays
+    e2e = e2e_solve(wl, dtype) if rank == 0 and not args.no_e2e else None
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        rate, dt = cpu_oracle_rate(wl, dtype, args.cpu_iters, os.cpu_count() or 1)
+        cpu = {'value': rate, 'unit': UNIT, 'cores': os.cpu_count() or 1, 'kind': 'port',
+               'sample': f'{args.cpu_iters} iterations of the numpy oracle on the full workload ({dt:.1f} s), '
+                         f'scipy.fft with {os.cpu_count()} workers'}
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_per_step, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic (seeded generator)',
+            'config': {**config_of(args, wl), 'parallelism': f'replicas x{world}'},
+            'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clocks.summary(),
+            'gpu_launches': launches_per_iter * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    sol._engine.close()
+
+
+def len_passes(wl) -> int:
+    d = len(wl['shape'])
+    return 1 if d == 1 else 2 * d - 1
+
+
+def e2e_solve(wl, dtype):
+    import torch
+    from macromax_b200 import Bound, Grid, Solution
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    bound = Bound(grid, thickness=wl['bound_thickness'])
+    sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                   source_distribution=wl['source'], bound=bound, dtype=dtype)
+    eng = sol._engine
+    chi_host = eng.chi.cpu().numpy()
+    src_host = eng.sources.cpu().numpy()
+    e0 = np.zeros((eng.ncomp, *wl['shape']), dtype=dtype)
+    pin = [torch.from_numpy(a).pin_memory() for a in (chi_host, src_host, e0)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.chi.copy_(pin[0], non_blocking=True)
+    eng.sources.copy_(pin[1], non_blocking=True)
+    eng.set_fields(pin[2])
+    st = eng.run(float(wl['rtol']), float(wl['maxiter']))
+    out = eng.current(st)[0].cpu().numpy()
+    dt = time.perf_counter() - t0
+    iters = int(st['iteration'][0])
+    h2d = sum(int(p.numel() * p.element_size()) for p in pin)
+    d2h = int(out.nbytes)
+    sol._engine.close()
+    return {'value': eng.N * iters / dt, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+            'iterations': iters, 'seconds': dt, 'residue': float(st['residue'][0]),
+            'step': f"one solve to residue {wl['rtol']} from host arrays"}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return {'hbm_gbs': float(d['hbm_gbs']), 'source': 'measured (MEASURED_PEAKS.json)'}
+    except (OSError, KeyError, ValueError):
+        return {'hbm_gbs': 6650.0, 'source': 'fallback 6.65 TB/s'}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='spheres3d')
+    ap.add_argument('--n', type=int, default=128)
+    ap.add_argument('--cpu-iters', type=int, default=6)
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = make_workload(args)
+    rank, world, local, pg = dist_setup(args)
+    try:
+        if args.impl == 'reference':
+            bench_reference(args, wl, rank, world, pg)
+        else:
+            bench_ours(args, wl, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,148 @@
+/*
+ * macromax_b200 -- C ABI of the B200-native split-Richardson (modified Born) solver.
+ *
+ * Every entry point takes plain pointers and sizes; device pointers are CUDA device memory of the device that was
+ * current when the plan was created, `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ * Functions return MMX_OK (0) on success and a negative code on failure; mmx_last_error() then describes the
+ * failure (thread-local, valid until the next call on the same thread).
+ *
+ * Data layout (C order, complex words interleaved re/im; complex64 = 8 bytes, complex128 = 16 bytes):
+ *   field  [batch][ncomp][n0][n1][n2]      ncomp = 1 (scalar) or 3 (vector); the reference's [c, 1, *grid]
+ *   chi    [m][n0][n1][n2]                  m = 1 (isotropic) or 9 (3x3, row-major); the reference's [r, r, *grid]
+ *   source [batch][ncomp][n0][n1][n2]      the preconditioned source s' = i s / (alpha_i beta)
+ * Each call replaces a call site of the reference MacroMax Python package (paths relative to python/macromax).
+ */
+#ifndef MACROMAX_B200_H
+#define MACROMAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MMX_OK 0
+#define MMX_ERR_ARG (-1)
+#define MMX_ERR_CUDA (-2)
+#define MMX_ERR_UNSUPPORTED (-3)
+
+#define MMX_C64 0  /* complex64 words  */
+#define MMX_C128 1 /* complex128 words */
+
+#define MMX_CHI_SCALAR 1 /* isotropic susceptibility, one word per voxel */
+#define MMX_CHI_MAT3 9   /* 3x3 susceptibility tensor, nine words per voxel */
+
+/* status codes of an mmx_rhs_state */
+#define MMX_STATUS_OK 0
+#define MMX_STATUS_ZERODIV 1 /* update norm 0 after a previous norm of 0: the reference raises ZeroDivisionError */
+
+/*
+ * Per right-hand-side iteration state, one entry per batch member, in DEVICE memory.  Mirrors the private state of
+ * Solution (solver.py:161, 474, 997-1047): alpha, previous_update_norm, iteration, residue.  chi and the source are
+ * stored once, at alpha0; the iteration applies chi(alpha) = chi0 alpha0_i / alpha_i + i (alpha0 - alpha) / alpha_i
+ * and s'(alpha) = s'0 alpha0_i / alpha_i on the fly, which is what __update_operators (solver.py:496-528) does to
+ * the stored arrays when the divergence guard raises alpha_i.
+ */
+typedef struct mmx_rhs_state {
+  double alpha_re, alpha_im;   /* current alpha */
+  double alpha0_re, alpha0_im; /* alpha at which chi and source were stored */
+  double prev_norm;            /* previous_update_norm, +inf after a reset (solver.py:161, 720, 832) */
+  double last_norm;            /* ||d|| of the last iteration */
+  double field_norm;           /* ||E|| of the current field (times k0^2) */
+  double residue;              /* previous_update_norm / ||E|| (solver.py:1026-1042) */
+  double rtol;                 /* keep iterating while residue > rtol ... */
+  double maxiter;              /* ... and iteration < maxiter (solver.py:81-83) */
+  int32_t iteration;           /* iterations since the last reset of the counter */
+  int32_t cur;                 /* which of the two field buffers holds the current E */
+  int32_t active;              /* 1 while the stop rule asks for more iterations */
+  int32_t accepted;            /* 1 if the last update was accepted by the divergence guard */
+  int32_t rejections;          /* number of rejected updates (alpha_i raised by 1.5x) */
+  int32_t status;              /* MMX_STATUS_* */
+  int32_t reserved[2];
+} mmx_rhs_state;
+
+typedef struct mmx_plan mmx_plan;
+
+/* Human-readable description of the last failure on this thread. */
+const char* mmx_last_error(void);
+
+/* ABI version of this library. */
+int mmx_version(void);
+
+/*
+ * Create a plan for fields on a periodic grid of `ndim` (1..3) axes with lengths `shape` (C order), `ncomp` (1|3)
+ * components, `batch` right-hand sides and word `precision` (MMX_C64 | MMX_C128) on the current CUDA device.
+ * Replaces the grid / dtype / working-array set-up of BackEnd.__init__ (backend/__init__.py:43-67) and
+ * backend.load (backend/__init__.py:922-1012).  Axis lengths must factor into 2, 3, 5, 7, 11, 13.
+ */
+int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int precision, mmx_plan** plan);
+
+/* Release a plan and its device memory (twiddles, k tables, work buffers). */
+int mmx_plan_destroy(mmx_plan* plan);
+
+/*
+ * Set the k-vectors of the k0-scaled grid: for each axis a, shape[a] values k_a[j] (origin at index 0), concatenated
+ * over the axes (host memory, FP64).  Replaces BackEnd.k (backend/__init__.py:651-656; utils/ft/grid.py:426-439).
+ */
+int mmx_plan_set_kvectors(mmx_plan* plan, const double* k);
+
+/*
+ * N-D discrete Fourier transform over the grid axes of `nbatch` contiguous fields of the plan's shape and precision
+ * (in == out allowed).  inverse = 0: forward, unscaled; inverse = 1: inverse scaled by 1/N, so that
+ * ift(ft(x)) == x.  Replaces BackEnd.ft / BackEnd.ift (backend/__init__.py:234-257; numpy backend
+ * backend/numpy.py:112-133; torch backend backend/torch.py:183-205).
+ */
+int mmx_fftn(mmx_plan* plan, const void* in, void* out, int64_t nbatch, int inverse, void* stream);
+
+/*
+ * ||x||_2 of `nwords` complex words of the given precision, accumulated in FP64, written to out_dev[0] (device).
+ * Uses the plan's scratch.  Replaces BackEnd.norm (backend/__init__.py:872-874; backend/torch.py:316-317).
+ */
+int mmx_norm(mmx_plan* plan, const void* x, int64_t nwords, int precision, double* out_dev, void* stream);
+
+/*
+ * Run `niter` iterations of Solution.__iter__ (solver.py:1049-1098) for every active right-hand side:
+ *   d = chi [G (chi E + s') - E],  accept E += d if ||d|| < previous_update_norm, else alpha_i *= 1.5,
+ * with G = IFFT g(k) FFT, g = -i alpha_i / (|k|^2 - alpha) for scalar fields and the transverse/longitudinal split
+ * g (1 - P_L) + (i alpha_i / alpha) P_L for vector fields (solver.py:564-584; backend/__init__.py:606-649).
+ * The current field of RHS b is buffer state[b].cur of (E0, E1); the update is written to the other buffer and the
+ * two swap roles on acceptance.  A right-hand side whose state is inactive is skipped (convergence mask).
+ * chi: chi_kind MMX_CHI_SCALAR or MMX_CHI_MAT3, shared by all right-hand sides.  All launches are asynchronous on
+ * `stream`; no host synchronisation happens inside.
+ */
+int mmx_iterate(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                mmx_rhs_state* state, int niter, void* stream);
+
+/*
+ * Mixed-precision defect of the FP64 outer loop, for a complex128 plan:
+ *   s_out = s'(alpha) + chi(alpha) x - G(alpha)^{-1} x       (complex128 in, complex64 out)
+ * which is the source for which the plain iteration's fixed point is the correction to x.  Uses state[b].alpha
+ * and the stored alpha0 as mmx_iterate does.  No reference counterpart: the reference iterates in one precision.
+ */
+int mmx_defect(mmx_plan* plan, const void* x, const void* chi, int chi_kind, const void* src,
+               const mmx_rhs_state* state, void* s_out, void* stream);
+
+/* x (complex128) += delta (complex64), `nwords` words.  Solution accumulation of the FP64 outer loop. */
+int mmx_accumulate(void* x, const void* delta, int64_t nwords, void* stream);
+
+/*
+ * Adjoint-state gradient of a real loss with respect to the permittivity, per voxel:
+ *   grad[b][v] = scale * conj( sum_c nu[b][c][v] * E[b][c][v] )   (isotropic, ncomp components)
+ * where nu solves the adjoint problem with source conj(dL/dE) (torch convention).  No reference counterpart.
+ */
+int mmx_adjoint_grad(const void* E, const void* nu, void* grad, int64_t batch, int ncomp, int64_t nvox,
+                     int precision, double scale, void* stream);
+
+/*
+ * Pointwise matrix product out = A B of matrix fields (BackEnd.mul, backend/__init__.py:415-444;
+ * backend/torch.py:220-249): A [ra][ca][N], B [ca][cb][N] (B's voxel stride 0 if b_broadcast), out [ra][cb][N].
+ */
+int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int b_broadcast, void* out,
+                      int64_t nvox, int precision, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MACROMAX_B200_H */

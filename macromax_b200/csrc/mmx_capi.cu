@@ -1,0 +1,625 @@
+// C ABI of macromax_b200: plans, launch configuration and the extern "C" entry points declared in
+// include/macromax_b200.h.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <algorithm>
+#include <vector>
+
+#include "mmx_fast.cuh"
+
+#define MMX_ABI_VERSION 1
+
+static_assert(sizeof(mmx_rhs_state) == 112, "mmx_rhs_state layout is part of the ABI");
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(MMX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define MMX_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+constexpr size_t kSmemCap = 220 * 1024;
+
+struct PassCfg {
+  int axis;
+  int ops;
+  int64_t outer, inner;
+  int P, sP, threads;
+  size_t smem;
+  int64_t tiles;
+  int fast = 0;  // 1: compile-time specialised kernel (complex64, N in the specialised set)
+};
+
+constexpr int kFastP = 8;
+bool fast_length(int n) { return n == 64 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512; }
+
+}  // namespace
+
+struct mmx_plan {
+  int device = 0;
+  int ndim = 0;
+  int64_t shape[3] = {1, 1, 1};
+  int ncomp = 1;
+  int batch = 1;
+  int prec = MMX_C64;
+  int64_t N = 1;
+  FFTAxis ax[3];           // radix plans; tw points at device twiddles of the plan precision
+  void* tw_dev[3] = {nullptr, nullptr, nullptr};
+  void* kv_dev = nullptr;  // k tables, plan precision, concatenated
+  int kv_off[3] = {0, 0, 0};
+  bool kv_set = false;
+  void* work = nullptr;    // T [batch][ncomp][N]
+  double* partials = nullptr;
+  int64_t partials_len = 0;
+  unsigned int* done = nullptr;  // per-RHS tile counters of the epilogue pass (zero between iterations)
+  std::vector<PassCfg> iter_passes;
+  std::vector<PassCfg> defect_passes;
+  bool force_generic = false;  // MMX_FORCE_GENERIC=1: use only the runtime-length kernels (tests)
+  // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
+  bool l2_persist = false;
+  size_t l2_window = 0;
+  size_t l2_prev_limit = 0;
+};
+
+namespace {
+
+bool factorize(int n, FFTAxis& ax) {
+  ax.n = n;
+  ax.nst = 0;
+  int m = n;
+  const int pref[] = {8, 4, 2, 3, 5, 7, 11, 13};
+  while (m > 1) {
+    bool found = false;
+    for (int r : pref) {
+      if (m % r == 0) {
+        if (ax.nst >= MMX_MAX_STAGES) return false;
+        ax.radix[ax.nst++] = r;
+        m /= r;
+        found = true;
+        break;
+      }
+    }
+    if (!found) return false;
+  }
+  return true;
+}
+
+size_t word_bytes(int prec) { return prec == MMX_C128 ? 16 : 8; }
+
+// Pencils per tile: as many as fit ~64 KB of shared memory (at least 4 consecutive strided pencils, i.e. one
+// 32-byte sector per row, when the row fits), bounded by the 512-thread launch bound of the pass kernels.
+void choose_tile(const FFTAxis& ax, int C, int64_t outer, int64_t inner, int prec, PassCfg& pc) {
+  const size_t wb = word_bytes(prec);
+  const size_t budget = 64 * 1024;
+  const int64_t npenc = outer * inner;
+  int P = 1;
+  auto smem_of = [&](int p) { return (size_t)C * ax.n * (size_t)(p > 1 ? p + 1 : 1) * wb; };
+  auto thr_of = [&](int p) { return fft_tile_threads(C, p, ax); };
+  const int pmax = (int)std::min<int64_t>(npenc, 64);
+  if (inner > 1) {
+    const int pmin = (int)std::min<int64_t>(inner, prec == MMX_C128 ? 2 : 4);
+    P = pmin;
+    while (P * 2 <= pmax && P * 2 <= inner && smem_of(P * 2) <= budget && thr_of(P * 2) <= 512) P *= 2;
+    while (P > 1 && (smem_of(P) > kSmemCap || thr_of(P) > 512)) P /= 2;
+  } else {
+    P = 1;
+    while (P * 2 <= pmax && smem_of(P * 2) <= budget && thr_of(P * 2) <= 512) P *= 2;
+  }
+  pc.P = P;
+  pc.sP = P > 1 ? P + 1 : 1;
+  int thr = thr_of(P);
+  thr = ((thr + 31) / 32) * 32;
+  if (thr < 64) thr = 64;
+  pc.threads = thr;
+  pc.smem = smem_of(P);
+  pc.tiles = (npenc + P - 1) / P;
+  pc.outer = outer;
+  pc.inner = inner;
+}
+
+template <class R, int C, int CHI, int OPS>
+int launch_iter(const PassCfg& pc, IterArgs<R> a, int batch, cudaStream_t s) {
+  auto kern = k_iter_pass<R, C, CHI, OPS>;
+  static int configured_mask = 0;  // per-device attribute set once (devices < 32)
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured_mask & (1 << dev))) {
+    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+    configured_mask |= (1 << dev);
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  a.P = pc.P;
+  a.sP = pc.sP;
+  dim3 grid((unsigned)pc.tiles, (unsigned)batch);
+  kern<<<grid, pc.threads, pc.smem, s>>>(a);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+template <class R, int C, int CHI>
+int dispatch_ops(const PassCfg& pc, const IterArgs<R>& a, int batch, cudaStream_t s) {
+  switch (pc.ops) {
+    case OP_PRO | OP_FWD: return launch_iter<R, C, CHI, OP_PRO | OP_FWD>(pc, a, batch, s);
+    case OP_FWD: return launch_iter<R, C, MMX_CHI_SCALAR, OP_FWD>(pc, a, batch, s);
+    case OP_FWD | OP_G | OP_INV: return launch_iter<R, C, MMX_CHI_SCALAR, OP_FWD | OP_G | OP_INV>(pc, a, batch, s);
+    case OP_INV: return launch_iter<R, C, MMX_CHI_SCALAR, OP_INV>(pc, a, batch, s);
+    case OP_INV | OP_EPI: return launch_iter<R, C, CHI, OP_INV | OP_EPI>(pc, a, batch, s);
+    case OP_PRO | OP_FWD | OP_G | OP_INV | OP_EPI:
+      return launch_iter<R, C, CHI, OP_PRO | OP_FWD | OP_G | OP_INV | OP_EPI>(pc, a, batch, s);
+    // defect pipeline (G^{-1})
+    case OP_XLOAD | OP_FWD: return launch_iter<R, C, MMX_CHI_SCALAR, OP_XLOAD | OP_FWD>(pc, a, batch, s);
+    case OP_FWD | OP_G | OP_GINV | OP_INV:
+      return launch_iter<R, C, MMX_CHI_SCALAR, OP_FWD | OP_G | OP_GINV | OP_INV>(pc, a, batch, s);
+    case OP_INV | OP_DEFECT: return launch_iter<R, C, CHI, OP_INV | OP_DEFECT>(pc, a, batch, s);
+    case OP_XLOAD | OP_FWD | OP_G | OP_GINV | OP_INV | OP_DEFECT:
+      return launch_iter<R, C, CHI, OP_XLOAD | OP_FWD | OP_G | OP_GINV | OP_INV | OP_DEFECT>(pc, a, batch, s);
+    default: return fail(MMX_ERR_ARG, "internal: unknown pass operation set");
+  }
+}
+
+template <int C, int CHI, int OPS, int N, bool STRIDED>
+int launch_fast(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  auto kern = k_fast_pass<C, CHI, OPS, N, kFastP, STRIDED>;
+  static int configured_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured_mask & (1 << dev))) {
+    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+    configured_mask |= (1 << dev);
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  a.P = kFastP;
+  a.sP = kFastP + 1;
+  dim3 grid((unsigned)pc.tiles, (unsigned)batch);
+  if (a.l2_window) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(FastThreads<C, N, kFastP>::value);
+    cfg.dynamicSmemBytes = pc.smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = (void*)a.T;
+    attr[0].val.accessPolicyWindow.num_bytes = a.l2_window;
+    attr[0].val.accessPolicyWindow.hitRatio = 1.0f;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    MMX_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
+  } else {
+    kern<<<grid, FastThreads<C, N, kFastP>::value, pc.smem, s>>>(a);
+  }
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+template <int C, int CHI, int N>
+int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_t s) {
+  switch (pc.ops) {
+    case OP_PRO | OP_FWD: return launch_fast<C, CHI, OP_PRO | OP_FWD, N, false>(pc, a, batch, s);
+    case OP_INV | OP_EPI: return launch_fast<C, CHI, OP_INV | OP_EPI, N, false>(pc, a, batch, s);
+    case OP_FWD: return launch_fast<C, MMX_CHI_SCALAR, OP_FWD, N, true>(pc, a, batch, s);
+    case OP_INV: return launch_fast<C, MMX_CHI_SCALAR, OP_INV, N, true>(pc, a, batch, s);
+    case OP_FWD | OP_G | OP_INV: return launch_fast<C, MMX_CHI_SCALAR, OP_FWD | OP_G | OP_INV, N, true>(pc, a, batch, s);
+    default: return fail(MMX_ERR_ARG, "internal: operation set without a specialised kernel");
+  }
+}
+
+template <int N>
+int fast_dispatch_n(const PassCfg& pc, const IterArgs<float>& a, int C, int chi_kind, int batch, cudaStream_t s) {
+  if (C == 1) return fast_ops<1, MMX_CHI_SCALAR, N>(pc, a, batch, s);
+  if (chi_kind == MMX_CHI_SCALAR) return fast_ops<3, MMX_CHI_SCALAR, N>(pc, a, batch, s);
+  return fast_ops<3, MMX_CHI_MAT3, N>(pc, a, batch, s);
+}
+
+int fast_dispatch(const PassCfg& pc, const IterArgs<float>& a, int C, int chi_kind, int batch, cudaStream_t s) {
+  switch (a.ax.n) {
+    case 64: return fast_dispatch_n<64>(pc, a, C, chi_kind, batch, s);
+    case 128: return fast_dispatch_n<128>(pc, a, C, chi_kind, batch, s);
+    case 192: return fast_dispatch_n<192>(pc, a, C, chi_kind, batch, s);
+    case 256: return fast_dispatch_n<256>(pc, a, C, chi_kind, batch, s);
+    case 384: return fast_dispatch_n<384>(pc, a, C, chi_kind, batch, s);
+    case 512: return fast_dispatch_n<512>(pc, a, C, chi_kind, batch, s);
+    default: return fail(MMX_ERR_ARG, "internal: no specialised kernel for this length");
+  }
+}
+
+template <class R>
+int dispatch_pass(const PassCfg& pc, const IterArgs<R>& a, int C, int chi_kind, int batch, cudaStream_t s) {
+  if constexpr (std::is_same<R, float>::value) {
+    if (pc.fast) {
+      if (C == 1 && chi_kind != MMX_CHI_SCALAR) return fail(MMX_ERR_ARG, "a 3x3 chi needs a 3-component field");
+      return fast_dispatch(pc, a, C, chi_kind, batch, s);
+    }
+  }
+  if (C == 1) {
+    if (chi_kind != MMX_CHI_SCALAR) return fail(MMX_ERR_ARG, "a 3x3 chi needs a 3-component field");
+    return dispatch_ops<R, 1, MMX_CHI_SCALAR>(pc, a, batch, s);
+  }
+  if (chi_kind == MMX_CHI_SCALAR) return dispatch_ops<R, 3, MMX_CHI_SCALAR>(pc, a, batch, s);
+  return dispatch_ops<R, 3, MMX_CHI_MAT3>(pc, a, batch, s);
+}
+
+// pass sequence of one application of chi G chi (iteration) or of the FP64 defect
+std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
+  std::vector<PassCfg> v;
+  const int d = p->ndim;
+  auto geom = [&](int axis, int ops) {
+    PassCfg pc;
+    pc.axis = axis;
+    pc.ops = ops;
+    int64_t outer = 1, inner = 1;
+    for (int i = 0; i < axis; ++i) outer *= p->shape[i];
+    for (int i = axis + 1; i < d; ++i) inner *= p->shape[i];
+    choose_tile(p->ax[axis], p->ncomp, outer, inner, p->prec, pc);
+    const int n = (int)p->shape[axis];
+    const bool ops_ok = !defect && d > 1;
+    const bool geom_ok = inner > 1 ? (inner % kFastP == 0) : (outer % kFastP == 0);
+    if (p->prec == MMX_C64 && fast_length(n) && ops_ok && geom_ok && !p->force_generic) {
+      pc.fast = 1;
+      pc.P = kFastP;
+      pc.sP = kFastP + 1;
+      pc.tiles = outer * inner / kFastP;
+      pc.smem = ((size_t)p->ncomp * n * (kFastP + 1) + n) * sizeof(float2);
+      pc.threads = 0;  // fixed by the specialisation
+    }
+    v.push_back(pc);
+  };
+  const int first = defect ? (OP_XLOAD | OP_FWD) : (OP_PRO | OP_FWD);
+  const int last = defect ? (OP_INV | OP_DEFECT) : (OP_INV | OP_EPI);
+  const int mid = defect ? (OP_FWD | OP_G | OP_GINV | OP_INV) : (OP_FWD | OP_G | OP_INV);
+  if (d == 1) {
+    geom(0, first | last | mid);
+    return v;
+  }
+  geom(d - 1, first);
+  for (int a = d - 2; a >= 1; --a) geom(a, OP_FWD);
+  geom(0, mid);
+  for (int a = 1; a <= d - 2; ++a) geom(a, OP_INV);
+  geom(d - 1, last);
+  return v;
+}
+
+template <class R> IterArgs<R> base_args(mmx_plan* p) {
+  IterArgs<R> a;
+  memset(&a, 0, sizeof(a));
+  a.N = p->N;
+  a.ndim = p->ndim;
+  for (int i = 0; i < 3; ++i) {
+    a.dims[i] = (int)p->shape[i];
+    a.kv[i] = p->kv_dev ? (const R*)p->kv_dev + p->kv_off[i] : nullptr;
+  }
+  a.T = (cpx<R>*)p->work;
+  a.partials = p->partials;
+  a.done = p->done;
+  a.l2_window = p->l2_persist ? p->l2_window : 0;
+  a.inv_total = (R)(1.0 / (double)p->N);
+  return a;
+}
+
+template <class R>
+int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                   mmx_rhs_state* st, int niter, cudaStream_t s) {
+  IterArgs<R> a = base_args<R>(p);
+  a.E0 = (cpx<R>*)E0;
+  a.E1 = (cpx<R>*)E1;
+  a.chi = (const cpx<R>*)chi;
+  a.src = (const cpx<R>*)src;
+  a.st = st;
+  // the accept/reject decision is taken by the last tile of the epilogue pass (no separate launch)
+  for (int it = 0; it < niter; ++it) {
+    for (const PassCfg& pc : p->iter_passes) {
+      a.ax = p->ax[pc.axis];
+      int rc = dispatch_pass<R>(pc, a, p->ncomp, chi_kind, p->batch, s);
+      if (rc != MMX_OK) return rc;
+    }
+  }
+  return MMX_OK;
+}
+
+template <class R> int run_fftn(mmx_plan* p, const void* in, void* out, int64_t nbatch, int inverse, cudaStream_t s) {
+  const int d = p->ndim;
+  const void* cur_in = in;
+  for (int k = 0; k < d; ++k) {
+    const int axis = d - 1 - k;  // contiguous axis first
+    int64_t outer = nbatch, inner = 1;
+    for (int i = 0; i < axis; ++i) outer *= p->shape[i];
+    for (int i = axis + 1; i < d; ++i) inner *= p->shape[i];
+    PassCfg pc;
+    choose_tile(p->ax[axis], 1, outer, inner, p->prec, pc);
+    FFTPassArgs<R> a;
+    a.ax = p->ax[axis];
+    a.outer = outer;
+    a.inner = inner;
+    a.P = pc.P;
+    a.sP = pc.sP;
+    a.in = (const cpx<R>*)cur_in;
+    a.out = (cpx<R>*)out;
+    a.scale = (R)((inverse && k == d - 1) ? 1.0 / (double)p->N : 1.0);
+    if (inverse) {
+      auto kern = k_fft_pass<R, +1>;
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+      kern<<<(unsigned)pc.tiles, pc.threads, pc.smem, s>>>(a);
+    } else {
+      auto kern = k_fft_pass<R, -1>;
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+      kern<<<(unsigned)pc.tiles, pc.threads, pc.smem, s>>>(a);
+    }
+    MMX_CUDA(cudaGetLastError());
+    cur_in = out;
+  }
+  return MMX_OK;
+}
+
+int grid_blocks(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mmx_last_error(void) { return g_last_error.c_str(); }
+
+int mmx_version(void) { return MMX_ABI_VERSION; }
+
+int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int precision, mmx_plan** out) {
+  if (!out) return fail(MMX_ERR_ARG, "plan output pointer is NULL");
+  *out = nullptr;
+  if (ndim < 1 || ndim > 3) return fail(MMX_ERR_UNSUPPORTED, "grids of 1 to 3 axes are supported");
+  if (!shape) return fail(MMX_ERR_ARG, "shape is NULL");
+  if (ncomp != 1 && ncomp != 3) return fail(MMX_ERR_ARG, "ncomp must be 1 or 3");
+  if (batch < 1 || batch > 65535) return fail(MMX_ERR_ARG, "batch must be in 1..65535");
+  if (precision != MMX_C64 && precision != MMX_C128) return fail(MMX_ERR_ARG, "precision must be MMX_C64 or MMX_C128");
+  mmx_plan* p = new mmx_plan();
+  cudaGetDevice(&p->device);
+  p->ndim = ndim;
+  p->ncomp = ncomp;
+  p->batch = batch;
+  p->prec = precision;
+  p->N = 1;
+  for (int i = 0; i < ndim; ++i) {
+    if (shape[i] < 1 || shape[i] > 16384) {
+      delete p;
+      return fail(MMX_ERR_UNSUPPORTED, "axis lengths must be in 1..16384");
+    }
+    p->shape[i] = shape[i];
+    p->N *= shape[i];
+    if (!factorize((int)shape[i], p->ax[i])) {
+      delete p;
+      return fail(MMX_ERR_UNSUPPORTED, "axis length " + std::to_string(shape[i]) +
+                                           " has a prime factor above 13 (not supported)");
+    }
+  }
+  for (int i = ndim; i < 3; ++i) p->shape[i] = 1;
+  const size_t wb = word_bytes(precision);
+  // twiddles exp(-2 pi i t / n), computed in FP64
+  int kv_total = 0;
+  for (int i = 0; i < ndim; ++i) {
+    const int n = (int)shape[i];
+    std::vector<double> twd(2 * (size_t)n);
+    for (int t = 0; t < n; ++t) {
+      const double ang = -2.0 * M_PI * (double)t / (double)n;
+      twd[2 * t] = std::cos(ang);
+      twd[2 * t + 1] = std::sin(ang);
+    }
+    cudaError_t e = cudaMalloc(&p->tw_dev[i], wb * n);
+    if (e != cudaSuccess) {
+      mmx_plan_destroy(p);
+      return cuda_fail(e, "cudaMalloc(twiddles)");
+    }
+    if (precision == MMX_C128) {
+      e = cudaMemcpy(p->tw_dev[i], twd.data(), wb * n, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float> twf(2 * (size_t)n);
+      for (size_t k = 0; k < twf.size(); ++k) twf[k] = (float)twd[k];
+      e = cudaMemcpy(p->tw_dev[i], twf.data(), wb * n, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+      mmx_plan_destroy(p);
+      return cuda_fail(e, "cudaMemcpy(twiddles)");
+    }
+    p->ax[i].tw = p->tw_dev[i];
+    p->kv_off[i] = kv_total;
+    kv_total += n;
+  }
+  cudaError_t e = cudaMalloc(&p->kv_dev, (wb / 2) * (size_t)kv_total);
+  if (e == cudaSuccess) e = cudaMemset(p->kv_dev, 0, (wb / 2) * (size_t)kv_total);
+  if (e == cudaSuccess) e = cudaMalloc(&p->work, wb * (size_t)batch * ncomp * p->N);
+  if (e != cudaSuccess) {
+    mmx_plan_destroy(p);
+    return cuda_fail(e, "cudaMalloc(plan buffers)");
+  }
+  {
+    const char* fg = getenv("MMX_FORCE_GENERIC");
+    p->force_generic = fg && fg[0] == '1';
+    const char* lp = getenv("MMX_L2_PERSIST");
+    if (lp && lp[0] == '1' && precision == MMX_C64) {
+      int maxp = 0, maxw = 0;
+      cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, p->device);
+      cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, p->device);
+      const size_t tbytes = wb * (size_t)batch * ncomp * p->N;
+      if (maxp > 0 && maxw > 0) {
+        cudaDeviceGetLimit(&p->l2_prev_limit, cudaLimitPersistingL2CacheSize);
+        const size_t want = std::min<size_t>((size_t)maxp, tbytes);
+        if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) {
+          p->l2_persist = true;
+          p->l2_window = std::min<size_t>(tbytes, (size_t)maxw);
+        }
+        cudaGetLastError();
+      }
+    }
+  }
+  p->iter_passes = build_passes(p, false);
+  p->defect_passes = build_passes(p, true);
+  int64_t maxt = 2048;
+  for (auto& pc : p->iter_passes) maxt = std::max<int64_t>(maxt, pc.tiles);
+  p->partials_len = (int64_t)batch * maxt * 2;
+  e = cudaMalloc(&p->partials, sizeof(double) * p->partials_len);
+  if (e == cudaSuccess) e = cudaMalloc(&p->done, sizeof(unsigned int) * batch);
+  if (e == cudaSuccess) e = cudaMemset(p->done, 0, sizeof(unsigned int) * batch);
+  if (e != cudaSuccess) {
+    mmx_plan_destroy(p);
+    return cuda_fail(e, "cudaMalloc(partials)");
+  }
+  for (auto& pc : p->iter_passes) {
+    if (pc.smem > kSmemCap || pc.threads > 512) {
+      mmx_plan_destroy(p);
+      return fail(MMX_ERR_UNSUPPORTED, "axis too long for the shared-memory FFT with this many components");
+    }
+  }
+  *out = p;
+  return MMX_OK;
+}
+
+int mmx_plan_destroy(mmx_plan* p) {
+  if (!p) return MMX_OK;
+  for (int i = 0; i < 3; ++i)
+    if (p->tw_dev[i]) cudaFree(p->tw_dev[i]);
+  if (p->kv_dev) cudaFree(p->kv_dev);
+  if (p->work) cudaFree(p->work);
+  if (p->partials) cudaFree(p->partials);
+  if (p->done) cudaFree(p->done);
+  if (p->l2_persist) {  // hand the persisting set-aside back
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, p->l2_prev_limit);
+    cudaGetLastError();
+  }
+  delete p;
+  return MMX_OK;
+}
+
+int mmx_plan_set_kvectors(mmx_plan* p, const double* k) {
+  if (!p || !k) return fail(MMX_ERR_ARG, "NULL plan or k");
+  int total = 0;
+  for (int i = 0; i < p->ndim; ++i) total += (int)p->shape[i];
+  if (p->prec == MMX_C128) {
+    MMX_CUDA(cudaMemcpy(p->kv_dev, k, sizeof(double) * total, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> kf(total);
+    for (int i = 0; i < total; ++i) kf[i] = (float)k[i];
+    MMX_CUDA(cudaMemcpy(p->kv_dev, kf.data(), sizeof(float) * total, cudaMemcpyHostToDevice));
+  }
+  p->kv_set = true;
+  return MMX_OK;
+}
+
+int mmx_fftn(mmx_plan* p, const void* in, void* out, int64_t nbatch, int inverse, void* stream) {
+  if (!p || !in || !out) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (nbatch < 1) return fail(MMX_ERR_ARG, "nbatch must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->prec == MMX_C128) return run_fftn<double>(p, in, out, nbatch, inverse, s);
+  return run_fftn<float>(p, in, out, nbatch, inverse, s);
+}
+
+int mmx_norm(mmx_plan* p, const void* x, int64_t nwords, int precision, double* out_dev, void* stream) {
+  if (!p || !x || !out_dev) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (nwords < 0) return fail(MMX_ERR_ARG, "negative size");
+  cudaStream_t s = (cudaStream_t)stream;
+  int blocks = grid_blocks(nwords, 256);
+  if (blocks > p->partials_len) blocks = (int)p->partials_len;
+  if (precision == MMX_C128)
+    k_norm_partials<double><<<blocks, 256, 0, s>>>((const double2*)x, nwords, p->partials);
+  else
+    k_norm_partials<float><<<blocks, 256, 0, s>>>((const float2*)x, nwords, p->partials);
+  MMX_CUDA(cudaGetLastError());
+  k_norm_final<<<1, 256, 0, s>>>(p->partials, blocks, out_dev);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+int mmx_iterate(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                mmx_rhs_state* state, int niter, void* stream) {
+  if (!p || !E0 || !E1 || !chi || !src || !state) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (chi_kind != MMX_CHI_SCALAR && chi_kind != MMX_CHI_MAT3) return fail(MMX_ERR_ARG, "unknown chi_kind");
+  if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
+  if (niter < 0) return fail(MMX_ERR_ARG, "negative iteration count");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->prec == MMX_C128) return run_iterations<double>(p, E0, E1, chi, chi_kind, src, state, niter, s);
+  return run_iterations<float>(p, E0, E1, chi, chi_kind, src, state, niter, s);
+}
+
+int mmx_defect(mmx_plan* p, const void* x, const void* chi, int chi_kind, const void* src, const mmx_rhs_state* st,
+               void* s_out, void* stream) {
+  if (!p || !x || !chi || !src || !st || !s_out) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (p->prec != MMX_C128) return fail(MMX_ERR_ARG, "mmx_defect needs a complex128 plan");
+  if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
+  cudaStream_t s = (cudaStream_t)stream;
+  IterArgs<double> a = base_args<double>(p);
+  a.E0 = (double2*)x;
+  a.E1 = (double2*)x;
+  a.chi = (const double2*)chi;
+  a.src = (const double2*)src;
+  a.st = st;
+  a.aux = (float2*)s_out;
+  for (const PassCfg& pc : p->defect_passes) {
+    a.ax = p->ax[pc.axis];
+    int rc = dispatch_pass<double>(pc, a, p->ncomp, chi_kind, p->batch, s);
+    if (rc != MMX_OK) return rc;
+  }
+  return MMX_OK;
+}
+
+int mmx_accumulate(void* x, const void* delta, int64_t nwords, void* stream) {
+  if (!x || !delta) return fail(MMX_ERR_ARG, "NULL buffer");
+  cudaStream_t s = (cudaStream_t)stream;
+  k_accumulate<<<grid_blocks(nwords, 256), 256, 0, s>>>((double2*)x, (const float2*)delta, nwords);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+int mmx_adjoint_grad(const void* E, const void* nu, void* grad, int64_t batch, int ncomp, int64_t nvox,
+                     int precision, double scale, void* stream) {
+  if (!E || !nu || !grad) return fail(MMX_ERR_ARG, "NULL buffer");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = grid_blocks(batch * nvox, 256);
+  if (precision == MMX_C128)
+    k_adjoint_grad<double><<<blocks, 256, 0, s>>>((const double2*)E, (const double2*)nu, (double2*)grad, batch, ncomp,
+                                                  nvox, scale);
+  else
+    k_adjoint_grad<float><<<blocks, 256, 0, s>>>((const float2*)E, (const float2*)nu, (float2*)grad, batch, ncomp,
+                                                 nvox, (float)scale);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int b_broadcast, void* out, int64_t nvox,
+                      int precision, void* stream) {
+  if (!A || !B || !out) return fail(MMX_ERR_ARG, "NULL buffer");
+  if (ra < 1 || ca < 1 || cb < 1 || ra > 3 || ca > 3 || cb > 3) return fail(MMX_ERR_ARG, "matrix dims must be 1..3");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = grid_blocks(nvox, 256);
+  const int bstride = b_broadcast ? 0 : 1;
+  if (precision == MMX_C128)
+    k_pointwise_mul<double><<<blocks, 256, 0, s>>>((const double2*)A, ra, ca, (const double2*)B, cb, bstride,
+                                                   (double2*)out, nvox);
+  else
+    k_pointwise_mul<float><<<blocks, 256, 0, s>>>((const float2*)A, ra, ca, (const float2*)B, cb, bstride,
+                                                  (float2*)out, nvox);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+}  // extern "C"

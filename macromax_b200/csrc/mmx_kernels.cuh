@@ -1,0 +1,464 @@
+// Device kernels of the split-Richardson iteration: fused FFT passes, the per-RHS accept/reject decision, norms
+// and pointwise helpers.
+//
+// One iteration d = chi [G (chi E + s') - E] (reference solver.py:1070-1075) is executed as one FFT pass per grid
+// axis and direction, each pass reading and writing every word once:
+//   1D: [PRO FWD G INV EPI]                         (one kernel)
+//   2D: [PRO FWD ax1] [FWD G INV ax0] [INV EPI ax1]
+//   3D: [PRO FWD ax2] [FWD ax1] [FWD G INV ax0] [INV ax1] [INV EPI ax2]
+// PRO = prologue T = chi E + s' on the load of the first pass; G = the Green multiply between the forward and the
+// inverse transform of axis 0 (all other axes are already in k-space there); EPI = epilogue of the last pass:
+// d = chi (T - E), E_new = E + d written to the other field buffer, with per-CTA partial sums of |d|^2 and |E_new|^2
+// reduced in a fixed order by the last tile of each right-hand side, which then takes the accept/reject decision.
+#pragma once
+#include "../../include/macromax_b200.h"
+#include "mmx_fft.cuh"
+
+enum : int {
+  OP_PRO = 1,      // prologue: T = chi(alpha) E + s'(alpha)
+  OP_FWD = 2,      // forward FFT along the pass axis
+  OP_G = 4,        // Green multiply (axis-0 pass only)
+  OP_INV = 8,      // inverse FFT along the pass axis
+  OP_EPI = 16,     // iteration epilogue: d = chi (T - E); E' = E + d; partial norms
+  OP_GINV = 32,    // with OP_G: apply G^{-1} instead of G
+  OP_XLOAD = 64,   // first pass of the defect: load x instead of T
+  OP_DEFECT = 128  // defect epilogue: s_out = s' + chi x - T, stored as complex64
+};
+
+template <class R> struct IterArgs {
+  FFTAxis ax;
+  int64_t outer, inner;  // pencil geometry of the pass axis (per component, per RHS)
+  int P, sP;             // pencils per tile, shared-memory row pitch
+  int64_t N;             // voxels per component
+  int ndim;
+  int dims[3];
+  const R* kv[3];        // k-vector tables per axis
+  cpx<R>* T;             // work [B][C][N]
+  cpx<R>* E0;            // field buffers [B][C][N] (E0 is x for the defect)
+  cpx<R>* E1;
+  const cpx<R>* chi;     // [m][N]
+  const cpx<R>* src;     // [B][C][N]
+  const mmx_rhs_state* st;
+  double* partials;      // [B][gridDim.x][2]
+  unsigned int* done;    // [B] tiles of the epilogue pass finished (reset by the last one)
+  R inv_total;           // 1 / N
+  float2* aux;           // defect output [B][C][N] complex64
+  size_t l2_window;      // bytes of T kept L2-resident (0: off); host-side launch attribute only
+};
+
+// |z|^2 accumulated in FP64 (the squares of complex64 words are exact in double)
+__device__ __forceinline__ double norm2d(float2 z) { return (double)z.x * z.x + (double)z.y * z.y; }
+__device__ __forceinline__ double norm2d(double2 z) { return z.x * z.x + z.y * z.y; }
+
+template <class R> struct ChiCoef {
+  cpx<R> a;   // chi(alpha) = a chi0 + b I
+  cpx<R> b;
+  R s;        // s'(alpha) = s s'0
+  R alpha_re, alpha_im;
+};
+
+template <class R> __device__ __forceinline__ ChiCoef<R> chi_coef(const mmx_rhs_state* st) {
+  // chi(alpha) = chi0 alpha0_i / alpha_i + i (alpha0 - alpha) / alpha_i ; s'(alpha) = s'0 alpha0_i / alpha_i
+  const double ai = st->alpha_im, ar = st->alpha_re;
+  const double ratio = st->alpha0_im / ai;
+  ChiCoef<R> c;
+  c.a = mkc<R>((R)ratio, (R)0);
+  // i (d_re + i d_im) / ai = (-d_im + i d_re) / ai
+  const double dre = st->alpha0_re - ar, dim = st->alpha0_im - ai;
+  c.b = mkc<R>((R)(-dim / ai), (R)(dre / ai));
+  c.s = (R)ratio;
+  c.alpha_re = (R)ar;
+  c.alpha_im = (R)ai;
+  return c;
+}
+
+__device__ __forceinline__ int64_t pencil_base(int64_t p, int64_t inner, int n) {
+  const int64_t o = p / inner;
+  return o * (int64_t)n * inner + (p - o * inner);
+}
+
+// chi(alpha) applied to the C-vector v at voxel vox: out_r = sum_s (a chi_rs + b delta_rs) v_s
+template <class R, int C, int CHI>
+__device__ __forceinline__ void apply_chi(const cpx<R>* __restrict__ chi, int64_t N, int64_t vox, const ChiCoef<R>& cc,
+                                          const cpx<R>* v, cpx<R>* out) {
+  if constexpr (CHI == MMX_CHI_SCALAR) {
+    const cpx<R> x = cc.a * chi[vox] + cc.b;
+#pragma unroll
+    for (int c = 0; c < C; ++c) out[c] = x * v[c];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      cpx<R> acc = cc.b * v[r];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) acc += (cc.a * chi[(r * 3 + s) * N + vox]) * v[s];
+      out[r] = acc;
+    }
+  }
+}
+
+template <class R>
+__device__ __forceinline__ void block_reduce_2(double x, double y, double* out2) {
+  __shared__ double red[2][32];
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_down_sync(full, x, o);
+    y += __shfl_down_sync(full, y, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][warp] = x;
+    red[1][warp] = y;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    x = lane < nw ? red[0][lane] : 0.0;
+    y = lane < nw ? red[1][lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(full, x, o);
+      y += __shfl_down_sync(full, y, o);
+    }
+    if (lane == 0) {
+      out2[0] = x;
+      out2[1] = y;
+    }
+  }
+}
+
+template <class R, int C, bool GINV>
+__device__ __forceinline__ void green_step(cpx<R>* sm, const IterArgs<R>& a, int64_t p0, int64_t np_total,
+                                           const ChiCoef<R>& cc) {
+  const int n = a.ax.n, P = a.P, sP = a.sP;
+  const R ar = cc.alpha_re, ai = cc.alpha_im;
+  // h = i alpha_i / alpha (longitudinal factor, solver.py:575)
+  const cpx<R> h = divc(mkc<R>((R)0, ai), mkc<R>(ar, ai));
+  for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+    const int pl = e % P;
+    const int j = e / P;
+    const int64_t p = p0 + pl;
+    if (p >= np_total) continue;
+    R k[3] = {(R)0, (R)0, (R)0};
+    k[0] = a.kv[0][j];
+    if (a.ndim == 3) {
+      const int i1 = (int)(p / a.dims[2]);
+      const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
+      k[1] = a.kv[1][i1];
+      k[2] = a.kv[2][i2];
+    } else if (a.ndim == 2) {
+      k[1] = a.kv[1][p];
+    }
+    const R k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+    // g = -i alpha_i / (|k|^2 - alpha)  (solver.py:566-568)
+    const cpx<R> den = mkc<R>(k2 - ar, -ai);
+    const cpx<R> g = divc(mkc<R>((R)0, -ai), den);
+    if constexpr (C == 1) {
+      const int idx = j * sP + pl;
+      if constexpr (GINV) sm[idx] = divc(sm[idx], g) * a.inv_total;
+      else sm[idx] = sm[idx] * (g * a.inv_total);
+    } else {
+      cpx<R> F[3], PL[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) F[c] = sm[(c * n + j) * sP + pl];
+      const bool origin = (j == 0) && (p == 0);
+      if (origin) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? F[c] : mkc<R>((R)0, (R)0);
+      } else {
+        cpx<R> proj = mkc<R>((R)0, (R)0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if (c < a.ndim) proj += k[c] * F[c];
+        proj = proj * ((R)1 / k2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? k[c] * proj : mkc<R>((R)0, (R)0);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cpx<R> r;
+        if constexpr (GINV) r = divc(F[c] - PL[c], g) + divc(PL[c], h);
+        else r = g * (F[c] - PL[c]) + h * PL[c];
+        sm[(c * n + j) * sP + pl] = r * a.inv_total;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+template <class R, int C, int CHI, int OPS>
+__global__ void __launch_bounds__(512, 2) k_iter_pass(IterArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  cpx<R>* sm = reinterpret_cast<cpx<R>*>(mmx_smem_raw);
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  if (!st->active) return;  // convergence mask: uniform over the block
+  const ChiCoef<R> cc = chi_coef<R>(st);
+  const int n = a.ax.n, P = a.P, sP = a.sP;
+  const int64_t N = a.N, inner = a.inner;
+  const int64_t np_total = a.outer * inner;
+  const int64_t p0 = (int64_t)blockIdx.x * P;
+  const int64_t fbase = (int64_t)b * C * N;
+  const bool contig = (inner == 1);
+  const int cur = st->cur;
+  cpx<R>* __restrict__ Ecur = cur ? a.E1 : a.E0;
+  cpx<R>* __restrict__ Eoth = cur ? a.E0 : a.E1;
+
+  // ---------------- load ----------------
+  if constexpr ((OPS & OP_PRO) != 0) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+      int j, pl;
+      if (contig) { j = e % n; pl = e / n; } else { pl = e % P; j = e / P; }
+      const int64_t p = p0 + pl;
+      cpx<R> t[C];
+      if (p < np_total) {
+        const int64_t vox = pencil_base(p, inner, n) + (int64_t)j * inner;
+        cpx<R> v[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c] = Ecur[fbase + c * N + vox];
+        apply_chi<R, C, CHI>(a.chi, N, vox, cc, v, t);
+#pragma unroll
+        for (int c = 0; c < C; ++c) t[c] += cc.s * a.src[fbase + c * N + vox];
+      } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) t[c] = mkc<R>((R)0, (R)0);
+      }
+#pragma unroll
+      for (int c = 0; c < C; ++c) sm[(c * n + j) * sP + pl] = t[c];
+    }
+  } else {
+    const cpx<R>* __restrict__ srcp = ((OPS & OP_XLOAD) != 0) ? a.E0 : a.T;
+#pragma unroll 8
+    for (int e = threadIdx.x; e < C * n * P; e += blockDim.x) {
+      int j, pl, c;
+      if (contig) { j = e % n; const int r = e / n; pl = r % P; c = r / P; }
+      else { pl = e % P; const int r = e / P; j = r % n; c = r / n; }
+      const int64_t p = p0 + pl;
+      cpx<R> v = mkc<R>((R)0, (R)0);
+      if (p < np_total) v = srcp[fbase + c * N + pencil_base(p, inner, n) + (int64_t)j * inner];
+      sm[(c * n + j) * sP + pl] = v;
+    }
+  }
+  __syncthreads();
+
+  // ---------------- transforms ----------------
+  if constexpr ((OPS & OP_FWD) != 0) fft_tile<R, -1>(sm, C, P, sP, a.ax);
+  if constexpr ((OPS & OP_G) != 0) green_step<R, C, (OPS & OP_GINV) != 0>(sm, a, p0, np_total, cc);
+  if constexpr ((OPS & OP_INV) != 0) fft_tile<R, +1>(sm, C, P, sP, a.ax);
+
+  // ---------------- store ----------------
+  if constexpr ((OPS & OP_EPI) != 0) {
+    double dd2 = 0.0, en2 = 0.0;
+    for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+      int j, pl;
+      if (contig) { j = e % n; pl = e / n; } else { pl = e % P; j = e / P; }
+      const int64_t p = p0 + pl;
+      if (p >= np_total) continue;
+      const int64_t vox = pencil_base(p, inner, n) + (int64_t)j * inner;
+      cpx<R> v[C], dd[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const cpx<R> ev = Ecur[fbase + c * N + vox];
+        v[c] = sm[(c * n + j) * sP + pl] - ev;  // G(chi E + s') - E
+        dd[c] = ev;                              // keep E for the update
+      }
+      cpx<R> d[C];
+      apply_chi<R, C, CHI>(a.chi, N, vox, cc, v, d);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const cpx<R> en = dd[c] + d[c];
+        Eoth[fbase + c * N + vox] = en;
+        dd2 += norm2d(d[c]);
+        en2 += norm2d(en);
+      }
+    }
+    finish_pass_norms(a, b, dd2, en2);
+  } else if constexpr ((OPS & OP_DEFECT) != 0) {
+    for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+      int j, pl;
+      if (contig) { j = e % n; pl = e / n; } else { pl = e % P; j = e / P; }
+      const int64_t p = p0 + pl;
+      if (p >= np_total) continue;
+      const int64_t vox = pencil_base(p, inner, n) + (int64_t)j * inner;
+      cpx<R> x[C], cx[C];
+#pragma unroll
+      for (int c = 0; c < C; ++c) x[c] = a.E0[fbase + c * N + vox];
+      apply_chi<R, C, CHI>(a.chi, N, vox, cc, x, cx);
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        const cpx<R> s = cc.s * a.src[fbase + c * N + vox] + cx[c] - sm[(c * n + j) * sP + pl];
+        a.aux[fbase + c * N + vox] = to_c32(s);
+      }
+    }
+  } else {
+    for (int e = threadIdx.x; e < C * n * P; e += blockDim.x) {
+      int j, pl, c;
+      if (contig) { j = e % n; const int r = e / n; pl = r % P; c = r / P; }
+      else { pl = e % P; const int r = e / P; j = r % n; c = r / n; }
+      const int64_t p = p0 + pl;
+      if (p < np_total) a.T[fbase + c * N + pencil_base(p, inner, n) + (int64_t)j * inner] = sm[(c * n + j) * sP + pl];
+    }
+  }
+}
+
+// Accept / reject of Solution.__iter__ (solver.py:1077-1096) and the stop rule of solve (solver.py:81-83,
+// 1112-1121) for one right-hand side, from the epilogue pass partials (deterministic fixed-order reduction).
+// Executed by one whole block.
+__device__ void decide_rhs(mmx_rhs_state* S, const double* __restrict__ pp, int ntiles) {
+  double dd2 = 0.0, en2 = 0.0;
+  for (int i = threadIdx.x; i < ntiles; i += blockDim.x) {
+    dd2 += pp[2 * i];
+    en2 += pp[2 * i + 1];
+  }
+  double out2[2];
+  block_reduce_2<double>(dd2, en2, out2);
+  if (threadIdx.x == 0) {
+    const double nu = sqrt(out2[0]);
+    S->iteration += 1;
+    S->last_norm = nu;
+    const double prev = S->prev_norm;
+    if (prev == 0.0) {  // Python float division by zero in solver.py:1079
+      S->status = MMX_STATUS_ZERODIV;
+      S->active = 0;
+      return;
+    }
+    const double rel = nu / prev;
+    if (rel < 1.0) {
+      S->cur ^= 1;
+      S->prev_norm = nu;
+      S->field_norm = sqrt(out2[1]);
+      S->accepted = 1;
+    } else {
+      S->alpha_im = 1.5 * S->alpha_im;  // solver.py:1092
+      S->rejections += 1;
+      S->accepted = 0;
+    }
+    S->residue = S->prev_norm > 0.0 ? S->prev_norm / S->field_norm : 0.0;
+    S->active = ((double)S->iteration < S->maxiter) && (S->residue > S->rtol);
+  }
+}
+
+__global__ void k_decide(mmx_rhs_state* states, const double* __restrict__ partials, int ntiles) {
+  mmx_rhs_state* S = states + blockIdx.x;
+  if (!S->active) return;
+  decide_rhs(S, partials + (int64_t)blockIdx.x * ntiles * 2, ntiles);
+}
+
+// End of the epilogue pass for one tile: publish the tile's partial norms; the last tile of the RHS to finish
+// (counted with an atomic after a fence, no waiting) reduces them in a fixed order and takes the decision.
+template <class R>
+__device__ __forceinline__ void finish_pass_norms(const IterArgs<R>& a, int b, double dd2, double en2) {
+  __shared__ int s_last;
+  double out2[2];
+  block_reduce_2<R>(dd2, en2, out2);
+  if (threadIdx.x == 0) {
+    double* dst = a.partials + ((int64_t)b * gridDim.x + blockIdx.x) * 2;
+    dst[0] = out2[0];
+    dst[1] = out2[1];
+    __threadfence();
+    const unsigned int prev = atomicAdd(a.done + b, 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    decide_rhs(const_cast<mmx_rhs_state*>(a.st) + b, a.partials + (int64_t)b * gridDim.x * 2, gridDim.x);
+    if (threadIdx.x == 0) a.done[b] = 0u;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Plain FFT pass (BackEnd.ft / ift): C = 1, batch folded into the outer dimension.
+// ------------------------------------------------------------------------------------------------------------
+template <class R> struct FFTPassArgs {
+  FFTAxis ax;
+  int64_t outer, inner;
+  int P, sP;
+  const cpx<R>* in;
+  cpx<R>* out;
+  R scale;
+};
+
+template <class R, int DIR> __global__ void __launch_bounds__(512, 2) k_fft_pass(FFTPassArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  cpx<R>* sm = reinterpret_cast<cpx<R>*>(mmx_smem_raw);
+  const int n = a.ax.n, P = a.P, sP = a.sP;
+  const int64_t inner = a.inner, np_total = a.outer * inner;
+  const int64_t p0 = (int64_t)blockIdx.x * P;
+  const bool contig = inner == 1;
+  for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+    int j, pl;
+    if (contig) { j = e % n; pl = e / n; } else { pl = e % P; j = e / P; }
+    const int64_t p = p0 + pl;
+    cpx<R> v = mkc<R>((R)0, (R)0);
+    if (p < np_total) v = a.in[pencil_base(p, inner, n) + (int64_t)j * inner];
+    sm[j * sP + pl] = v;
+  }
+  __syncthreads();
+  fft_tile<R, DIR>(sm, 1, P, sP, a.ax);
+  for (int e = threadIdx.x; e < n * P; e += blockDim.x) {
+    int j, pl;
+    if (contig) { j = e % n; pl = e / n; } else { pl = e % P; j = e / P; }
+    const int64_t p = p0 + pl;
+    if (p < np_total) a.out[pencil_base(p, inner, n) + (int64_t)j * inner] = sm[j * sP + pl] * a.scale;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// Norms and pointwise kernels
+// ------------------------------------------------------------------------------------------------------------
+template <class R> __global__ void k_norm_partials(const cpx<R>* __restrict__ x, int64_t n, double* partials) {
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += norm2d(x[i]);
+  double out2[2];
+  block_reduce_2<R>(s, 0.0, out2);
+  if (threadIdx.x == 0) partials[blockIdx.x] = out2[0];
+}
+
+__global__ void k_norm_final(const double* __restrict__ partials, int np, double* out) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+  double out2[2];
+  block_reduce_2<double>(s, 0.0, out2);
+  if (threadIdx.x == 0) out[0] = sqrt(out2[0]);
+}
+
+__global__ void k_accumulate(double2* __restrict__ x, const float2* __restrict__ d, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 v = d[i];
+    double2 y = x[i];
+    y.x += (double)v.x;
+    y.y += (double)v.y;
+    x[i] = y;
+  }
+}
+
+template <class R>
+__global__ void k_adjoint_grad(const cpx<R>* __restrict__ E, const cpx<R>* __restrict__ nu, cpx<R>* __restrict__ g,
+                               int64_t batch, int ncomp, int64_t nvox, R scale) {
+  const int64_t total = batch * nvox;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = i / nvox, v = i - b * nvox;
+    cpx<R> acc = mkc<R>((R)0, (R)0);
+    for (int c = 0; c < ncomp; ++c) {
+      const int64_t idx = (b * ncomp + c) * nvox + v;
+      acc += nu[idx] * E[idx];
+    }
+    g[i] = conjc(acc) * scale;
+  }
+}
+
+template <class R>
+__global__ void k_pointwise_mul(const cpx<R>* __restrict__ A, int ra, int ca, const cpx<R>* __restrict__ B, int cb,
+                                int bstride, cpx<R>* __restrict__ out, int64_t nvox) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
+    for (int r = 0; r < ra; ++r)
+      for (int q = 0; q < cb; ++q) {
+        cpx<R> acc = mkc<R>((R)0, (R)0);
+        for (int s = 0; s < ca; ++s) acc += A[(r * ca + s) * nvox + v] * B[(s * cb + q) * (bstride ? nvox : 1) + (bstride ? v : 0)];
+        out[(r * cb + q) * nvox + v] = acc;
+      }
+  }
+}

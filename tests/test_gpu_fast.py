@@ -1,0 +1,74 @@
+"""
+The compile-time specialised pass kernels (complex64, axis lengths 64..512) against the runtime-length kernels and
+against the numpy oracle at sizes where the specialised path is taken.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _solution(wl, dtype=np.complex64, generic=False):
+    from macromax_b200 import Bound, Grid, Solution
+    old = os.environ.get('MMX_FORCE_GENERIC')
+    os.environ['MMX_FORCE_GENERIC'] = '1' if generic else '0'
+    try:
+        grid = Grid(shape=wl['shape'], step=wl['step'])
+        return Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                        source_distribution=wl['source'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                        dtype=dtype)
+    finally:
+        if old is None:
+            os.environ.pop('MMX_FORCE_GENERIC', None)
+        else:
+            os.environ['MMX_FORCE_GENERIC'] = old
+
+
+def rel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(np.asarray(b).ravel()))
+
+
+def _cases():
+    from macromax_b200 import workloads as w
+    return {
+        'spheres3d_64': lambda: w.spheres_3d(n=64, nb_spheres=40),
+        'design3d_64': lambda: w.design_3d(n=64),
+        'disks2d_128': lambda: w.disks_2d(n=128),
+        'disks2d_256': lambda: w.disks_2d(n=256),
+        'voronoi3d_64': lambda: w.voronoi_3d(n=64, nb_grains=12, boundary_px=48),
+        'mixed_3d': lambda: {**w.design_3d(n=64), 'shape': (64, 40, 64),
+                             'epsilon': w.design_3d(n=64)['epsilon'][:, :40, :],
+                             'source': w.design_3d(n=64)['source'][:, :, :40, :]},
+    }
+
+
+@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_128', 'disks2d_256', 'voronoi3d_64',
+                                  'mixed_3d'])
+def test_specialised_matches_generic(name):
+    wl = _cases()[name]()
+    fast = _solution(wl)
+    gen = _solution(wl, generic=True)
+    fast.solve(None, rtol=0, maxiter=15)
+    gen.solve(None, rtol=0, maxiter=15)
+    assert fast.iteration == gen.iteration == 15
+    assert rel(fast.E, gen.E) < 2e-6
+
+
+@pytest.mark.parametrize('name', ['spheres3d_64', 'disks2d_256'])
+def test_specialised_matches_oracle(name):
+    from oracle import mmoracle as mo
+    wl = _cases()[name]()
+    sol = _solution(wl)
+    ref = mo.from_workload(wl, np.complex128)
+    assert abs(sol.alpha - ref.alpha) <= 1e-9 * abs(ref.alpha)
+    rec_ref = ref.solve(rtol=0, maxiter=20, record=(1, 5, 20))
+    fields = {}
+    for s in sol:
+        if s.iteration in (1, 5, 20):
+            fields[s.iteration] = s.E
+        if s.iteration >= 20:
+            break
+    for it in (1, 5, 20):
+        assert rel(fields[it], rec_ref[it]) < 1e-5, (it, rel(fields[it], rec_ref[it]))
