@@ -116,9 +116,10 @@ int mmx_iterate(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kin
 
 /*
  * Mixed-precision defect of the FP64 outer loop, for a complex128 plan:
- *   s_out = s'(alpha) + chi(alpha) x - G(alpha)^{-1} x       (complex128 in, complex64 out)
- * which is the source for which the plain iteration's fixed point is the correction to x.  Uses state[b].alpha
- * and the stored alpha0 as mmx_iterate does.  No reference counterpart: the reference iterates in one precision.
+ *   s_out = [s'(alpha) + chi(alpha) x - G(alpha)^{-1} x] alpha_i / alpha0_i      (complex128 in, complex64 out)
+ * i.e. the source, normalised to alpha0 like every stored source, for which the plain iteration's fixed point is
+ * the correction to x.  Uses state[b].alpha and alpha0 as mmx_iterate does.  No reference counterpart: the
+ * reference iterates in one precision.
  */
 int mmx_defect(mmx_plan* plan, const void* x, const void* chi, int chi_kind, const void* src,
                const mmx_rhs_state* state, void* s_out, void* stream);

@@ -1,0 +1,101 @@
+"""
+Adjoint-state gradient of the solve behind ``torch.autograd.Function``.
+
+The converged field satisfies A E = s / k0^2 with A = -laplacian - eps (k0-scaled units; for vector fields the
+curl-curl operator): this is the fixed point of the preconditioned iteration (reference solver.py:1070-1075,
+E = G (chi E + s') with chi = i (eps - alpha) / alpha_i, s' = i s / alpha_i, g = -i alpha_i / (k^2 - alpha)).  A is
+complex symmetric for isotropic (and for symmetric anisotropic) permittivity, so for a real loss L with torch
+gradient g = dL/dRe(E) + i dL/dIm(E):
+
+    nu = A^{-1} conj(g)          -- the same fused solve with source conj(g), same material and alpha
+    dL/d eps = conj(sum_c nu_c E_c)           (k0^2-scaled fields; fused kernel mmx_adjoint_grad)
+    dL/d s   = conj(nu) / k0^2
+
+No iteration history is stored: the backward pass needs only the forward field and one adjoint field.  The
+reference has no adjoint; its only gradient path back-propagates through an unrolled torch restatement of the
+iteration (examples/scattering_neural_network.py:206-300).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .batch import BatchSolution
+from .grid import Grid
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    s = torch.cuda.current_stream().cuda_stream
+    return ctypes.c_void_p(s) if s else None
+
+
+class _SolveFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, epsilon, sources, problem):
+        grid, k0 = problem['grid'], problem['wavenumber']
+        eps_np = epsilon.detach().cpu().numpy()
+        src_np = sources.detach().cpu().numpy()
+        bs = BatchSolution(grid, src_np, eps_np, bound=problem.get('bound'), wavenumber=k0,
+                           dtype=problem.get('dtype', np.complex64), device=sources.device)
+        bs.solve(problem.get('rtol', 1e-6), problem.get('maxiter', 100000))
+        problem.setdefault('stats', {})['forward_iterations'] = bs.iterations
+        E = bs.E_device.clone()  # [B, C, N], k0^2-scaled
+        ctx.bs = bs
+        ctx.problem = problem
+        ctx.eps_is_complex = torch.is_complex(epsilon)
+        ctx.eps_shape = epsilon.shape
+        ctx.save_for_backward(E)
+        return (E * (1.0 / k0 ** 2)).reshape(bs.batch, bs.ncomp, *(int(n) for n in grid.shape))
+
+    @staticmethod
+    def backward(ctx, grad_E):
+        (E,) = ctx.saved_tensors
+        bs, problem = ctx.bs, ctx.problem
+        k0 = problem['wavenumber']
+        B, C, N = bs.batch, bs.ncomp, bs.engine.N
+        g = grad_E.detach().reshape(B, C, N)
+        # adjoint solve A nu = conj(g): the engine's field F for source s satisfies A F = s, so the source conj(g)
+        # gives nu directly.  It starts again from alpha0: the forward solve may have raised alpha (divergence
+        # guard), and the fixed point does not depend on alpha.
+        bs.engine.set_sources(torch.conj(g).to(bs.engine.torch_dtype) * (1.0j / bs.pre.alpha.imag / bs.pre.beta))
+        bs.engine.reset_alpha()
+        bs.engine.reset_update_norm()
+        bs.set_fields(0.0)
+        bs.solve(problem.get('rtol', 1e-6), problem.get('maxiter', 100000))
+        problem['stats']['adjoint_iterations'] = bs.iterations
+        nu = bs.E_device  # [B, C, N]
+        grad_eps = grad_src = None
+        if ctx.needs_input_grad[0]:
+            gb = torch.empty((B, N), dtype=E.dtype, device=E.device)
+            nat.call('mmx_adjoint_grad', _ptr(E), _ptr(nu), _ptr(gb), B, C, N,
+                     nat.MMX_C64 if E.dtype == torch.complex64 else nat.MMX_C128, 1.0, _stream())
+            # E is k0^2-scaled, the returned field is E / k0^2: dE_phys = A^{-1}(d eps E_phys)
+            gsum = gb.sum(dim=0).reshape(tuple(int(n) for n in bs.grid.shape)) * (1.0 / k0 ** 2)
+            grad_eps = gsum if ctx.eps_is_complex else gsum.real
+            grad_eps = grad_eps.reshape(ctx.eps_shape)
+        if ctx.needs_input_grad[1]:
+            grad_src = (torch.conj(nu) * (1.0 / k0 ** 2)).reshape(B, C, *(int(n) for n in bs.grid.shape))
+        bs.close()
+        return grad_eps, grad_src, None
+
+
+def solve(epsilon: torch.Tensor, sources: torch.Tensor, grid: Grid, wavenumber: float, bound=None,
+          dtype=np.complex64, rtol: float = 1e-6, maxiter: int = 100000, stats: dict | None = None) -> torch.Tensor:
+    """
+    Differentiable solve: E [B, 1|3, *grid] for the isotropic permittivity ``epsilon`` [*grid] (real or complex)
+    and sources [B, 1|3, *grid] (``source_distribution`` units).  Gradients flow to epsilon and sources through the
+    adjoint solve above.
+    """
+    problem = dict(grid=grid, wavenumber=float(wavenumber), bound=bound, dtype=dtype, rtol=rtol, maxiter=maxiter)
+    if stats is not None:
+        problem['stats'] = stats
+    if sources.dim() == grid.ndim + 1:
+        sources = sources.unsqueeze(0)
+    return _SolveFn.apply(epsilon, sources, problem)

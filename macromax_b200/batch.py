@@ -1,0 +1,143 @@
+"""
+Many right-hand sides sharing one material, solved together on the device.
+
+The reference solves one source at a time: ``ScatteringMatrix`` (matrix.py:770-844) loops over its columns and
+re-runs ``Solution.solve`` (matrix.py:650-669) with a new ``source_distribution`` on one shared ``Solution``, so every
+column has the same alpha and chi.  ``BatchSolution`` keeps that contract -- one preconditioner built from the
+material, B sources -- and iterates all B sources in the same kernel launches: the field layout is
+[B][components][grid], chi is stored once, and every right-hand side carries its own state (alpha after
+divergence-guard rejections, previous update norm, iteration count, residue).  The stop rule
+``iteration < maxiter and residue > rtol`` is evaluated per right-hand side after every iteration on the device; a
+finished right-hand side is masked out of later launches (its tiles return immediately), so each one stops at
+exactly the iteration where its own sequential solve would stop.
+"""
+from __future__ import annotations
+
+from math import inf
+
+import numpy as np
+import scipy.constants as const
+
+from . import _native as nat
+from . import preconditioner as pc
+from .bound import Bound, Electric, PeriodicBound
+from .engine import IterationEngine
+from .grid import Grid
+
+
+def _to_matrix_field(arr, ndim):
+    arr = np.asarray(arr)
+    while arr.ndim < ndim + 2:
+        arr = arr[np.newaxis]
+    if arr.shape[0] == 1 and arr.shape[1] > 1:
+        arr = arr.swapaxes(0, 1)
+    return arr
+
+
+def prepare_material(grid: Grid, epsilon, bound: Bound | None, wavenumber: float, dtype):
+    """Permittivity (plus an Electric bound's susceptibility) as a matrix field, and its preconditioner."""
+    bound = bound if bound is not None else PeriodicBound(grid)
+    eps = _to_matrix_field(np.asarray(epsilon, dtype=np.complex128), grid.ndim)
+    if isinstance(bound, Electric):
+        chi_b = np.asarray(bound.electric_susceptibility)
+        if eps.shape[0] > 1:
+            chi_b = np.eye(3).reshape(3, 3, *([1] * grid.ndim)) * chi_b
+        eps = eps + chi_b
+    pre = pc.prepare(eps, bound.thickness, wavenumber, float(np.finfo(np.dtype(dtype)).eps))
+    return pre, bound
+
+
+class BatchSolution:
+    """
+    B sources [B, 1|3, *grid] (``source_distribution`` units, i.e. i omega mu0 J) in one material.
+    ``E`` is [B, 1|3, *grid]; ``iterations``, ``residues``, ``rejections`` and ``alphas`` are per source.
+    """
+
+    def __init__(self, grid: Grid, sources, epsilon, bound: Bound | None = None, vacuum_wavelength=None,
+                 wavenumber=None, dtype=np.complex64, device=None, preconditioner=None):
+        if not isinstance(grid, Grid):
+            grid = Grid.from_ranges(*grid)
+        self.grid = grid
+        self.wavenumber = 2 * np.pi / vacuum_wavelength if vacuum_wavelength is not None else float(wavenumber)
+        self.dtype = np.dtype(dtype)
+        src = np.asarray(sources)
+        if src.ndim == grid.ndim + 1:
+            src = src[np.newaxis]
+        if src.ndim != grid.ndim + 2:
+            raise ValueError('sources must be [B, 1|3, *grid]')
+        self.batch = src.shape[0]
+        self.ncomp = src.shape[1]
+        if self.ncomp not in (1, 3):
+            raise ValueError('sources need 1 or 3 components')
+        if preconditioner is None:
+            self.pre, self.bound = prepare_material(grid, epsilon, bound, self.wavenumber, self.dtype)
+        else:
+            self.pre, self.bound = preconditioner, bound
+        if self.pre.chi.shape[0] > 1 and self.ncomp != 3:
+            raise ValueError('an anisotropic permittivity needs vector sources')
+        self.engine = IterationEngine(grid.shape, self.ncomp, self.batch, self.dtype, (grid * self.wavenumber).k,
+                                      self.pre.chi, self.pre.alpha, device=device)
+        self.set_sources(src)
+
+    @property
+    def alpha0(self) -> complex:
+        return self.pre.alpha
+
+    def set_sources(self, src):
+        """s'0 = i s / (alpha0_i beta) (solver.py:702-720); resets every previous_update_norm."""
+        src = np.asarray(src)
+        self.engine.set_sources(src * (1.0j / self.pre.alpha.imag / self.pre.beta))
+        self.engine.reset_update_norm()
+
+    def set_fields(self, E=0.0):
+        E = np.broadcast_to(np.asarray(E), (self.batch, self.ncomp, *self.grid.shape))
+        self.engine.set_fields(E * self.wavenumber ** 2)
+
+    def solve(self, rtol: float = 1e-6, maxiter=inf) -> 'BatchSolution':
+        st = self.engine.run(float(rtol), float(maxiter))
+        if np.any(st['status'] == nat.MMX_STATUS_ZERODIV):
+            raise ZeroDivisionError('float division by zero (update norm after a zero update norm)')
+        self._state = st
+        return self
+
+    def iterate(self, n: int):
+        st = self.engine.read_state()
+        st['rtol'] = -1.0
+        st['maxiter'] = np.inf
+        st['active'] = 1
+        self.engine.write_state(st)
+        self.engine.iterate(n)
+
+    @property
+    def state(self) -> np.ndarray:
+        return self.engine.read_state()
+
+    @property
+    def iterations(self) -> np.ndarray:
+        return self.state['iteration'].copy()
+
+    @property
+    def residues(self) -> np.ndarray:
+        return self.state['residue'].copy()
+
+    @property
+    def rejections(self) -> np.ndarray:
+        return self.state['rejections'].copy()
+
+    @property
+    def alphas(self) -> np.ndarray:
+        st = self.state
+        return st['alpha_re'] + 1j * st['alpha_im']
+
+    @property
+    def E_device(self):
+        """Current fields (times k0^2) [B, C, N] on the device."""
+        return self.engine.current()
+
+    @property
+    def E(self) -> np.ndarray:
+        f = self.engine.current().cpu().numpy().reshape(self.batch, self.ncomp, *self.grid.shape)
+        return (f / self.wavenumber ** 2).astype(self.dtype)
+
+    def close(self):
+        self.engine.close()

@@ -287,8 +287,9 @@ __global__ void __launch_bounds__(512, 2) k_iter_pass(IterArgs<R> a) {
       apply_chi<R, C, CHI>(a.chi, N, vox, cc, x, cx);
 #pragma unroll
       for (int c = 0; c < C; ++c) {
+        // s'(alpha) + chi(alpha) x - G(alpha)^{-1} x, stored normalised to alpha0 like every source (/ s)
         const cpx<R> s = cc.s * a.src[fbase + c * N + vox] + cx[c] - sm[(c * n + j) * sP + pl];
-        a.aux[fbase + c * N + vox] = to_c32(s);
+        a.aux[fbase + c * N + vox] = to_c32(s * ((R)1 / cc.s));
       }
     }
   } else {

@@ -114,6 +114,14 @@ class IterationEngine:
         raw = np.ascontiguousarray(st, dtype=nat.STATE_DTYPE).view(np.uint8).reshape(self.batch, -1)
         self.state.copy_(torch.from_numpy(raw.copy()).to(self.device))
 
+    def reset_alpha(self, index=None):
+        """Return alpha to alpha0 (the stored chi and sources), e.g. before solving a new, unrelated problem."""
+        st = self.read_state()
+        sel = slice(None) if index is None else index
+        st['alpha_re'][sel] = st['alpha0_re'][sel]
+        st['alpha_im'][sel] = st['alpha0_im'][sel]
+        self.write_state(st)
+
     def reset_update_norm(self, index=None):
         st = self.read_state()
         sel = slice(None) if index is None else index

@@ -1,0 +1,142 @@
+"""
+Mixed-precision solve: complex64 inner iterations inside an FP64 defect-correction loop.
+
+The plain iteration's fixed point solves (G^{-1} - chi) E = s' (all at the current alpha; reference
+solver.py:1070-1075 with E = G (chi E + s')).  For an FP64 iterate x the defect
+
+    r(x) = s' + chi x - G^{-1} x                                  (FP64 on the device: one FFT pair, mmx_defect)
+
+is a source for which the plain iteration converges to the correction delta = x* - x.  So each outer step casts
+r(x) to complex64, runs the unchanged fused complex64 iteration from delta = 0 until its own residue falls below
+``inner_rtol``, and accumulates x += delta in FP64 (mmx_accumulate).  The first inner update from delta = 0 is
+d(x) = chi G r(x), the update the plain iteration would make at x, so ||d(x)|| / ||x|| is the relative residue of
+the outer iterate (the reference's residue, solver.py:1026-1042, evaluated at x).  Divergence-guard rejections in
+an inner solve raise alpha for that right-hand side; the defect of the next outer step is taken at that alpha, so
+both levels stay consistent.  FP64 is used only for the defect, the norms and the accumulated solution.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .batch import BatchSolution, prepare_material
+from .grid import Grid
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    s = torch.cuda.current_stream().cuda_stream
+    return ctypes.c_void_p(s) if s else None
+
+
+class MixedSolution:
+    def __init__(self, grid: Grid, sources, epsilon, bound=None, vacuum_wavelength=None, wavenumber=None,
+                 device=None):
+        if not isinstance(grid, Grid):
+            grid = Grid.from_ranges(*grid)
+        self.grid = grid
+        self.wavenumber = 2 * np.pi / vacuum_wavelength if vacuum_wavelength is not None else float(wavenumber)
+        pre, bound = prepare_material(grid, epsilon, bound, self.wavenumber, np.complex128)
+        src = np.asarray(sources)
+        if src.ndim == grid.ndim + 1:
+            src = src[np.newaxis]
+        self.inner = BatchSolution(grid, np.zeros_like(src), None, bound=bound, wavenumber=self.wavenumber,
+                                   dtype=np.complex64, device=device, preconditioner=pre)
+        self.pre = pre
+        self.batch, self.ncomp = self.inner.batch, self.inner.ncomp
+        eng = self.inner.engine
+        self.device = eng.device
+        N = eng.N
+        with torch.cuda.device(self.device):
+            self.plan64 = nat.Plan(grid.shape, self.ncomp, self.batch, nat.MMX_C128)
+            self.plan64.set_kvectors([np.asarray(k, dtype=np.float64).ravel() for k in (grid * self.wavenumber).k])
+            m = pre.chi.shape[0] * pre.chi.shape[1]
+            chi = np.broadcast_to(pre.chi, (pre.chi.shape[0], pre.chi.shape[1], *grid.shape)).reshape(m, N)
+            self.chi64 = torch.from_numpy(np.array(chi, dtype=np.complex128)).to(self.device)
+            s0 = src.reshape(self.batch, self.ncomp, N) * (1.0j / pre.alpha.imag / pre.beta)
+            self.src64 = torch.from_numpy(np.array(s0, dtype=np.complex128)).to(self.device)
+            self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
+            self._norm = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self.outer_residues = []
+        self.inner_iterations = []
+
+    def _xnorm(self, b):
+        nat.call('mmx_norm', self.plan64.handle, _ptr(self.x[b]), self.ncomp * self.inner.engine.N, nat.MMX_C128,
+                 _ptr(self._norm), _stream())
+        return float(self._norm.item())
+
+    def solve(self, rtol: float = 1e-8, inner_rtol: float = 1e-4, inner_maxiter: int = 100000, max_outer: int = 30):
+        eng = self.inner.engine
+        done = np.zeros(self.batch, dtype=bool)
+        for _ in range(max_outer):
+            # every unconverged right-hand side is active for the defect and for one first correction step
+            eng.set_fields(torch.zeros((self.batch, self.ncomp, eng.N), dtype=eng.torch_dtype, device=self.device))
+            st = eng.read_state()
+            st['iteration'] = 0
+            st['rtol'] = -1.0
+            st['maxiter'] = 1
+            st['active'] = (~done).astype(np.int32)
+            st['status'] = 0
+            eng.write_state(st)
+            nat.call('mmx_defect', self.plan64.handle, _ptr(self.x), _ptr(self.chi64), eng.chi_kind, _ptr(self.src64),
+                     _ptr(eng.state), _ptr(eng.sources), _stream())
+            eng.iterate(1)  # first correction step: its update norm is ||d(x)||
+            st = eng.read_state()
+            res = np.full(self.batch, np.inf)
+            for b in range(self.batch):
+                xn = self._xnorm(b)
+                if xn > 0:
+                    res[b] = st['last_norm'][b] / xn
+            res[done] = 0.0
+            self.outer_residues.append(res.copy())
+            newly = (res < rtol) & ~done
+            done |= newly
+            if np.all(done):
+                break
+            # finish the inner solves of the unconverged right-hand sides
+            st['iteration'] = 1
+            st['rtol'] = inner_rtol
+            st['maxiter'] = inner_maxiter
+            st['active'] = (~done).astype(np.int32)
+            eng.write_state(st)
+            chunk = 8
+            while True:
+                eng.iterate(chunk)
+                st = eng.read_state()
+                if not np.any(st['active']):
+                    break
+                chunk = min(2 * chunk, 64)
+            self.inner_iterations.append(st['iteration'].copy())
+            delta = eng.current(st)
+            for b in range(self.batch):
+                if not done[b]:
+                    nat.call('mmx_accumulate', _ptr(self.x[b]), _ptr(delta[b]), self.ncomp * eng.N, _stream())
+        self.converged = done
+        return self
+
+    @property
+    def residues(self) -> np.ndarray:
+        return self.outer_residues[-1] if self.outer_residues else np.full(self.batch, np.inf)
+
+    @property
+    def alphas(self) -> np.ndarray:
+        return self.inner.alphas
+
+    @property
+    def E(self) -> np.ndarray:
+        """FP64 solution [B, C, *grid] (divided by k0^2)."""
+        return (self.x.cpu().numpy() / self.wavenumber ** 2).reshape(self.batch, self.ncomp, *self.grid.shape)
+
+    @property
+    def total_inner_iterations(self) -> int:
+        return int(sum(int(np.max(i)) for i in self.inner_iterations)) + len(self.outer_residues)
+
+    def close(self):
+        self.plan64.close()
+        self.inner.close()
