@@ -142,6 +142,21 @@ int mmx_adjoint_grad(const void* E, const void* nu, void* grad, int64_t batch, i
 int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int b_broadcast, void* out,
                       int64_t nvox, int precision, void* stream);
 
+/*
+ * mmx_fftn without a plan and without any device allocation: the same transform as mmx_fftn (forward unscaled,
+ * inverse scaled by 1/N) over the `ndim` grid axes `shape` of `nbatch` contiguous fields of the given precision.
+ * No counterpart in the reference (which always allocates through its backend).  For callers that must not let a
+ * library allocate or free device memory: applications that place every buffer through their own pool or fixed
+ * memory plan (a serving process with a set memory budget, a framework's caching allocator), where a stray
+ * cudaMalloc can fail on a fully committed GPU and a cudaFree stalls the whole device while other streams run.
+ * Limits: every axis length at most 4096 and factorisable into 2, 3, 5, 7, 11, 13 (longer axes are rejected with
+ * MMX_ERR_UNSUPPORTED).  The twiddle scratch is one 192 KiB __device__ array shared by all calls in the process:
+ * calls that overlap on the GPU race; the first call on a device looks up that array's address and should be made
+ * before any stream capture.
+ */
+int mmx_fftn_noalloc(int ndim, const int64_t* shape, const void* in, void* out, int64_t nbatch, int inverse,
+                     int precision, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,7 +36,7 @@ assert STATE_DTYPE.itemsize == 112
 
 EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destroy', 'mmx_plan_set_kvectors',
             'mmx_fftn', 'mmx_norm', 'mmx_iterate', 'mmx_defect', 'mmx_accumulate', 'mmx_adjoint_grad',
-            'mmx_pointwise_mul']
+            'mmx_pointwise_mul', 'mmx_fftn_noalloc']
 
 _lib = None
 
@@ -71,6 +71,7 @@ def load(path: str | None = None):
         'mmx_accumulate': (i32, [vp, vp, i64, vp]),
         'mmx_adjoint_grad': (i32, [vp, vp, vp, i64, i32, i64, i32, dbl, vp]),
         'mmx_pointwise_mul': (i32, [vp, i32, i32, vp, i32, i32, vp, i64, i32, vp]),
+        'mmx_fftn_noalloc': (i32, [i32, ctypes.POINTER(i64), vp, vp, i64, i32, i32, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -7,6 +7,7 @@
 #include <string>
 #include <type_traits>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "mmx_fast.cuh"
@@ -623,3 +624,90 @@ int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------
+// Allocation-free N-D FFT.
+//
+// The twiddle tables that a plan would allocate live in one file-scope device array instead, sized for three axes
+// of at most MMX_NOALLOC_MAX_AXIS samples in complex128 (192 KiB, held by every GPU that loads this library until
+// the process exits).  Each call rewrites the tables it needs for its own shape on its stream before the transform
+// passes, so nothing has to start at zero; two calls that overlap on the GPU (different streams) overwrite each
+// other's tables and race.  In host code the array's name is only a stand-in for the device symbol: the device
+// address comes from cudaGetSymbolAddress, looked up once per device (on that device's first call).
+// ---------------------------------------------------------------------------------------------------------------
+#define MMX_NOALLOC_MAX_AXIS 4096
+
+static __device__ __align__(256) unsigned char g_noalloc_twiddles[3 * MMX_NOALLOC_MAX_AXIS * sizeof(double2)];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+void* g_noalloc_twiddle_ptr[kNoallocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+
+template <class R> __global__ void k_fill_twiddles(cpx<R>* __restrict__ tw, int n) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(-2.0 * (double)t / (double)n, &s, &c);  // exp(-2 pi i t / n)
+    tw[t] = mkc<R>((R)c, (R)s);
+  }
+}
+
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  MMX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices) return fail(MMX_ERR_UNSUPPORTED, "device ordinal too large");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_twiddle_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_twiddles);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_twiddles)");
+    g_noalloc_twiddle_ptr[dev] = p;
+  }
+  *out = g_noalloc_twiddle_ptr[dev];
+  return MMX_OK;
+}
+
+template <class R>
+int fftn_noalloc(mmx_plan& desc, unsigned char* scratch, const void* in, void* out, int64_t nbatch, int inverse,
+                 cudaStream_t s) {
+  for (int i = 0; i < desc.ndim; ++i) {
+    cpx<R>* tw = reinterpret_cast<cpx<R>*>(scratch + (size_t)i * MMX_NOALLOC_MAX_AXIS * sizeof(double2));
+    const int n = (int)desc.shape[i];
+    k_fill_twiddles<R><<<(n + 255) / 256, 256, 0, s>>>(tw, n);
+    MMX_CUDA(cudaGetLastError());
+    desc.ax[i].tw = tw;
+  }
+  return run_fftn<R>(&desc, in, out, nbatch, inverse, s);
+}
+
+}  // namespace
+
+extern "C" int mmx_fftn_noalloc(int ndim, const int64_t* shape, const void* in, void* out, int64_t nbatch,
+                                int inverse, int precision, void* stream) {
+  if (ndim < 1 || ndim > 3) return fail(MMX_ERR_UNSUPPORTED, "grids of 1 to 3 axes are supported");
+  if (!shape || !in || !out) return fail(MMX_ERR_ARG, "NULL shape or buffer");
+  if (nbatch < 1) return fail(MMX_ERR_ARG, "nbatch must be positive");
+  if (precision != MMX_C64 && precision != MMX_C128) return fail(MMX_ERR_ARG, "precision must be MMX_C64 or MMX_C128");
+  mmx_plan desc;  // host-side descriptor only: no device memory is attached to it
+  desc.ndim = ndim;
+  desc.prec = precision;
+  desc.N = 1;
+  for (int i = 0; i < ndim; ++i) {
+    if (shape[i] < 1 || shape[i] > MMX_NOALLOC_MAX_AXIS)
+      return fail(MMX_ERR_UNSUPPORTED, "axis length " + std::to_string(shape[i]) +
+                                           " exceeds the " + std::to_string(MMX_NOALLOC_MAX_AXIS) +
+                                           "-sample limit of the allocation-free FFT (use mmx_fftn with a plan)");
+    if (!factorize((int)shape[i], desc.ax[i]))
+      return fail(MMX_ERR_UNSUPPORTED, "axis length " + std::to_string(shape[i]) +
+                                           " has a prime factor above 13 (not supported)");
+    desc.shape[i] = shape[i];
+    desc.N *= shape[i];
+  }
+  void* scratch = nullptr;
+  const int rc = noalloc_scratch(&scratch);
+  if (rc != MMX_OK) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (precision == MMX_C128) return fftn_noalloc<double>(desc, (unsigned char*)scratch, in, out, nbatch, inverse, s);
+  return fftn_noalloc<float>(desc, (unsigned char*)scratch, in, out, nbatch, inverse, s);
+}
