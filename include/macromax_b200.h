@@ -36,6 +36,7 @@ extern "C" {
 /* status codes of an mmx_rhs_state */
 #define MMX_STATUS_OK 0
 #define MMX_STATUS_ZERODIV 1 /* update norm 0 after a previous norm of 0: the reference raises ZeroDivisionError */
+#define MMX_STATUS_TIMEOUT 2 /* a bounded wait for an asynchronous shared-memory copy gave up (results kept valid) */
 
 /*
  * Per right-hand-side iteration state, one entry per batch member, in DEVICE memory.  Mirrors the private state of

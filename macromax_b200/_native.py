@@ -23,6 +23,7 @@ MMX_CHI_SCALAR = 1
 MMX_CHI_MAT3 = 9
 MMX_STATUS_OK = 0
 MMX_STATUS_ZERODIV = 1
+MMX_STATUS_TIMEOUT = 2
 
 # numpy mirror of struct mmx_rhs_state (include/macromax_b200.h)
 STATE_DTYPE = np.dtype([

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "mmx_fast.cuh"
+#include "mmx_reg.cuh"
 
 #define MMX_ABI_VERSION 1
 
@@ -45,7 +46,13 @@ struct PassCfg {
   size_t smem;
   int64_t tiles;
   int fast = 0;  // 1: compile-time specialised kernel (complex64, N in the specialised set)
+  int reg = 0;   // 1: register-staged strided pass (k_reg_pass, 16-pencil tiles)
+  int regc = 0;  // 1: register-staged contiguous prologue/epilogue pass (k_regc_pass) for an isotropic chi
+  int64_t rc_tiles = 0;
+  size_t rc_smem = 0;
 };
+
+bool reg_length(int n, int C) { return C == 3 ? (n == 64 || n == 128) : (n == 64 || n == 128 || n == 256 || n == 512); }
 
 constexpr int kFastP = 8;
 bool fast_length(int n) { return n == 64 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512; }
@@ -72,6 +79,7 @@ struct mmx_plan {
   std::vector<PassCfg> iter_passes;
   std::vector<PassCfg> defect_passes;
   bool force_generic = false;  // MMX_FORCE_GENERIC=1: use only the runtime-length kernels (tests)
+  bool no_reg = false;         // MMX_NO_REG=1: shared-memory staged kernels for the strided passes (tests)
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
   size_t l2_window = 0;
@@ -213,8 +221,70 @@ int launch_fast(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   return MMX_OK;
 }
 
+template <int C, int OPS, int N>
+int launch_reg(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  if constexpr ((C == 3 && N > 128) || N == 192 || N == 384) {
+    return fail(MMX_ERR_ARG, "internal: no register-staged kernel for this length");
+  } else {
+    auto kern = k_reg_pass<C, OPS, N>;
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured_mask & (1 << dev))) {
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+        configured_mask |= (1 << dev);
+    }
+    a.outer = pc.outer;
+    a.inner = pc.inner;
+    a.P = kRegP;
+    a.sP = kRegP;
+    dim3 grid((unsigned)pc.tiles, (unsigned)batch);
+    kern<<<grid, RegThreads<C, N>::value, pc.smem, s>>>(a);
+    MMX_CUDA(cudaGetLastError());
+    return MMX_OK;
+  }
+}
+
+template <int C, int OPS, int N>
+int launch_regc(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  if constexpr (N == 192 || N == 384 || (C == 3 && N > 128)) {
+    return fail(MMX_ERR_ARG, "internal: no register-staged contiguous kernel for this length");
+  } else {
+    constexpr int PCK = (OPS & OP_EPI) ? RegCDefault<C, N>::PC_EPI : RegCDefault<C, N>::PC;
+    auto kern = k_regc_pass<C, OPS, N, PCK>;
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured_mask & (1 << dev))) {
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+        configured_mask |= (1 << dev);
+    }
+    a.outer = pc.outer;
+    a.inner = pc.inner;
+    dim3 grid((unsigned)pc.rc_tiles, (unsigned)batch);
+    kern<<<grid, RegC<C, N, PCK>::THREADS, pc.rc_smem, s>>>(a);
+    MMX_CUDA(cudaGetLastError());
+    return MMX_OK;
+  }
+}
+
 template <int C, int CHI, int N>
 int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_t s) {
+  if (pc.regc && CHI == MMX_CHI_SCALAR) {
+    switch (pc.ops) {
+      case OP_PRO | OP_FWD: return launch_regc<C, OP_PRO | OP_FWD, N>(pc, a, batch, s);
+      case OP_INV | OP_EPI: return launch_regc<C, OP_INV | OP_EPI, N>(pc, a, batch, s);
+      default: break;
+    }
+  }
+  if (pc.reg) {
+    switch (pc.ops) {
+      case OP_FWD: return launch_reg<C, OP_FWD, N>(pc, a, batch, s);
+      case OP_INV: return launch_reg<C, OP_INV, N>(pc, a, batch, s);
+      case OP_FWD | OP_G | OP_INV: return launch_reg<C, OP_FWD | OP_G | OP_INV, N>(pc, a, batch, s);
+      default: return fail(MMX_ERR_ARG, "internal: operation set without a register-staged kernel");
+    }
+  }
   switch (pc.ops) {
     case OP_PRO | OP_FWD: return launch_fast<C, CHI, OP_PRO | OP_FWD, N, false>(pc, a, batch, s);
     case OP_INV | OP_EPI: return launch_fast<C, CHI, OP_INV | OP_EPI, N, false>(pc, a, batch, s);
@@ -282,6 +352,33 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
       pc.tiles = outer * inner / kFastP;
       pc.smem = ((size_t)p->ncomp * n * (kFastP + 1) + n) * sizeof(float2);
       pc.threads = 0;  // fixed by the specialisation
+      const bool strided_op = ops == OP_FWD || ops == OP_INV || ops == (OP_FWD | OP_G | OP_INV);
+      const bool contig_op = ops == (OP_PRO | OP_FWD) || ops == (OP_INV | OP_EPI);
+      if (contig_op && inner == 1 && reg_length(n, p->ncomp) && !p->no_reg) {
+        const bool epi = (ops & OP_EPI) != 0;
+        int pcr = 1;
+        switch (n * 4 + p->ncomp) {
+          case 64 * 4 + 1: pcr = epi ? RegCDefault<1, 64>::PC_EPI : RegCDefault<1, 64>::PC; break;
+          case 128 * 4 + 1: pcr = epi ? RegCDefault<1, 128>::PC_EPI : RegCDefault<1, 128>::PC; break;
+          case 256 * 4 + 1: pcr = epi ? RegCDefault<1, 256>::PC_EPI : RegCDefault<1, 256>::PC; break;
+          case 512 * 4 + 1: pcr = epi ? RegCDefault<1, 512>::PC_EPI : RegCDefault<1, 512>::PC; break;
+          case 64 * 4 + 3: pcr = epi ? RegCDefault<3, 64>::PC_EPI : RegCDefault<3, 64>::PC; break;
+          case 128 * 4 + 3: pcr = epi ? RegCDefault<3, 128>::PC_EPI : RegCDefault<3, 128>::PC; break;
+        }
+        if (outer % pcr == 0) {
+          pc.regc = 1;
+          pc.rc_tiles = outer / pcr;
+          pc.rc_smem = ((size_t)p->ncomp * pcr * (n + n / 16) + n) * sizeof(float2);
+          if (epi) pc.rc_smem += (size_t)(p->ncomp + 1) * pcr * n * sizeof(float2);  // staged E and chi
+        }
+      }
+      if (strided_op && inner % kRegP == 0 && reg_length(n, p->ncomp) && !p->no_reg) {
+        pc.reg = 1;
+        pc.P = kRegP;
+        pc.sP = kRegP;
+        pc.tiles = outer * inner / kRegP;
+        pc.smem = ((size_t)p->ncomp * n * kRegP + n) * sizeof(float2);
+      }
     }
     v.push_back(pc);
   };
@@ -456,6 +553,8 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
   {
     const char* fg = getenv("MMX_FORCE_GENERIC");
     p->force_generic = fg && fg[0] == '1';
+    const char* nr = getenv("MMX_NO_REG");
+    p->no_reg = nr && nr[0] == '1';
     const char* lp = getenv("MMX_L2_PERSIST");
     if (lp && lp[0] == '1' && precision == MMX_C64) {
       int maxp = 0, maxw = 0;

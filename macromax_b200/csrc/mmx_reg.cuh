@@ -1,0 +1,463 @@
+// Register-staged FFT passes along a strided axis (the middle passes of the 3D schedule and the axis-0 pass with
+// the Green multiply), complex64, power-of-two lengths 64 .. 512.
+//
+// Same self-sorting stage formulation as mmx_fft.cuh, but the first radix stage reads its butterfly inputs
+// straight from global memory into registers and the last stage writes its outputs straight back, so a forward (or
+// inverse) pass exchanges data through shared memory only between stages.  A tile is 16 consecutive pencils of one
+// outer index; shared memory is laid out [c][j][pencil] with a 16-word (128-byte) row, and every warp covers two
+// whole rows in every access, which is conflict-free for 8-byte words.  Thread t works on pencil t % 16, butterfly
+// slot (t / 16) % TPP and component t / (16 TPP); a stage with T butterflies per pencil gives each thread T / TPP of
+// them.  Global accesses are 16 consecutive words (128 bytes) per row and warp.
+#pragma once
+#include "mmx_kernels.cuh"
+
+template <int... Rs> struct RegPlanList {};
+template <int N> struct RegPlan;
+template <> struct RegPlan<64> { using type = RegPlanList<8, 8>; static constexpr int TPP = 8; };
+template <> struct RegPlan<128> { using type = RegPlanList<16, 8>; static constexpr int TPP = 8; };
+template <> struct RegPlan<256> { using type = RegPlanList<16, 16>; static constexpr int TPP = 16; };
+template <> struct RegPlan<512> { using type = RegPlanList<8, 8, 8>; static constexpr int TPP = 32; };
+
+constexpr int kRegP = 16;
+
+template <int C, int N> struct RegThreads {
+  static constexpr int value = C * kRegP * RegPlan<N>::TPP;
+};
+
+// one stage; SRC/DST: 0 = shared memory, 1 = global memory (tile-relative, row stride jstride words)
+template <int DIR, int N, int C, int RAD, int L, bool FROM_G, bool TO_G>
+__device__ __forceinline__ void rstage(float2* __restrict__ sm, const float2* __restrict__ tw, const float2* gsrc,
+                                       float2* gdst, int64_t jstride, int64_t cstride) {
+  constexpr int P = kRegP;
+  constexpr int TPP = RegPlan<N>::TPP;
+  constexpr int T = N / RAD;
+  constexpr int NBT = T / TPP;
+  static_assert(NBT >= 1 && T % TPP == 0, "stage does not split evenly over the threads");
+  constexpr int TSTRIDE = N / (L * RAD);
+  const int tid = threadIdx.x;
+  const int pl = tid % P;
+  const int rest = tid / P;
+  const int ii = rest % TPP;
+  const int c = rest / TPP;
+  float2 u[NBT][RAD];
+#pragma unroll
+  for (int m = 0; m < NBT; ++m) {
+    const int i = ii + m * TPP;
+    const int kk = i % L;
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) {
+      const int j = i + q * T;
+      if constexpr (FROM_G) u[m][q] = gsrc[c * cstride + (int64_t)j * jstride + pl];
+      else u[m][q] = sm[(c * N + j) * P + pl];
+    }
+    if constexpr (L > 1) {
+#pragma unroll
+      for (int q = 1; q < RAD; ++q) {
+        float2 w = tw[q * kk * TSTRIDE];
+        if (DIR > 0) w = conjc(w);
+        u[m][q] = u[m][q] * w;
+      }
+    }
+    bfly<float, RAD, DIR>(u[m], tw, N);
+  }
+  if constexpr (!FROM_G && !TO_G) __syncthreads();  // in-place shared stage: all reads before any write
+#pragma unroll
+  for (int m = 0; m < NBT; ++m) {
+    const int i = ii + m * TPP;
+    const int kk = i % L;
+    const int d0 = (i - kk) * RAD + kk;
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) {
+      const int j = d0 + q * L;
+      if constexpr (TO_G) gdst[c * cstride + (int64_t)j * jstride + pl] = u[m][q];
+      else sm[(c * N + j) * P + pl] = u[m][q];
+    }
+  }
+  if constexpr (!TO_G) __syncthreads();
+}
+
+// all stages of one transform; FIRST_G: first stage reads global; LAST_G: last stage writes global
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, int R0, int... Rs>
+__device__ __forceinline__ void rstages(float2* sm, const float2* tw, const float2* gsrc, float2* gdst, int64_t js,
+                                        int64_t cs) {
+  constexpr bool last = sizeof...(Rs) == 0;
+  rstage<DIR, N, C, R0, L, FIRST_G, LAST_G && last>(sm, tw, gsrc, gdst, js, cs);
+  if constexpr (!last) rstages<DIR, N, C, false, LAST_G, L * R0, Rs...>(sm, tw, gsrc, gdst, js, cs);
+}
+
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int... Rs>
+__device__ __forceinline__ void rfft(float2* sm, const float2* tw, const float2* gsrc, float2* gdst, int64_t js,
+                                     int64_t cs, RegPlanList<Rs...>) {
+  rstages<DIR, N, C, FIRST_G, LAST_G, 1, Rs...>(sm, tw, gsrc, gdst, js, cs);
+}
+
+// OPS: OP_FWD (forward pass), OP_INV (inverse pass) or OP_FWD | OP_G | OP_INV (axis-0 pass with the Green multiply)
+template <int C, int OPS, int N>
+__global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArgs<float> a) {
+  constexpr int P = kRegP;
+  constexpr int THREADS = RegThreads<C, N>::value;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * N * P;
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  if (!st->active) return;
+  const int tid = threadIdx.x;
+  const int64_t inner = a.inner;
+  const int64_t p0 = (int64_t)blockIdx.x * P;
+  const int64_t o = p0 / inner;
+  const int64_t in0 = p0 - o * inner;
+  float2* tile = a.T + (int64_t)b * C * a.N + o * (int64_t)N * inner + in0;
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  __syncthreads();
+  using Plan = typename RegPlan<N>::type;
+  if constexpr (OPS == OP_FWD) {
+    rfft<-1, N, C, true, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
+  } else if constexpr (OPS == OP_INV) {
+    rfft<+1, N, C, true, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
+  } else {
+    // forward transform into shared memory, Green multiply, inverse transform back to global memory
+    rfft<-1, N, C, true, false>(sm, smtw, tile, tile, inner, a.N, Plan{});
+    const ChiCoef<float> cc = chi_coef<float>(st);
+    __shared__ float sk1[P], sk2[P], sk0[N];
+    if (tid < P) {
+      const int64_t p = in0 + tid;
+      float k1 = 0.f, k2 = 0.f;
+      if (a.ndim == 3) {
+        const int i1 = (int)(p / a.dims[2]);
+        const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
+        k1 = a.kv[1][i1];
+        k2 = a.kv[2][i2];
+      } else if (a.ndim == 2) {
+        k1 = a.kv[1][p];
+      }
+      sk1[tid] = k1;
+      sk2[tid] = k2;
+    }
+    for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
+    __syncthreads();
+    const float ar = cc.alpha_re, ai = cc.alpha_im;
+    const float2 hs = divc(make_float2(0.f, ai), make_float2(ar, ai)) * a.inv_total;
+    const float ai2s = ai * ai * a.inv_total, ais = -ai * a.inv_total;
+    for (int e = tid; e < N * P; e += THREADS) {
+      const int pl = e % P;
+      const int j = e / P;
+      const float k0 = sk0[j], k1 = sk1[pl], k2 = sk2[pl];
+      const float kk2 = k0 * k0 + k1 * k1 + k2 * k2;
+      const float dr = kk2 - ar;
+      const float inv = 1.f / (dr * dr + ai * ai);
+      const float2 g = make_float2(ai2s * inv, ais * dr * inv);  // -i a_i / (|k|^2 - a) / N
+      if constexpr (C == 1) {
+        sm[j * P + pl] = sm[j * P + pl] * g;
+      } else {
+        float2 F[3], PL[3];
+        const float kv[3] = {k0, k1, k2};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) F[c] = sm[(c * N + j) * P + pl];
+        if (j == 0 && in0 + pl == 0) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? F[c] : make_float2(0.f, 0.f);
+        } else {
+          float2 proj = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            if (c < a.ndim) proj += kv[c] * F[c];
+          proj = proj * (1.f / kk2);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? kv[c] * proj : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sm[(c * N + j) * P + pl] = g * (F[c] - PL[c]) + hs * PL[c];
+      }
+    }
+    __syncthreads();
+    rfft<+1, N, C, false, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Register-staged passes along the contiguous axis with the fused prologue / epilogue (isotropic chi).
+//
+// A tile is PC consecutive rows (pencils of N contiguous samples).  Thread t works on butterfly slot t % TPP,
+// row (t / TPP) % PC and component t / (TPP PC), so consecutive threads touch consecutive samples of a row in the
+// first-stage loads and the last-stage stores.  Shared memory is [c][row][N + N/16] with sample m stored at
+// m + m/16: with that skew the stride-RAD scatter of a stage and the unit-stride gather of the next one both hit
+// every bank pair exactly twice per warp (the minimum for 8-byte words).
+//   PRO | FWD: x = chi(alpha) E + s'(alpha) computed as the first stage loads it; forward FFT; T written back.
+//   INV | EPI: inverse FFT of T; the last stage produces the transformed samples in registers and applies
+//              d = chi(alpha)(T - E), E' = E + d, with FP64 partial norms, directly against global memory.
+// ---------------------------------------------------------------------------------------------------------------
+template <int C, int N> struct RegCDefault {
+  static constexpr int TPP = RegPlan<N>::TPP;
+  static constexpr int P0 = 384 / (C * TPP);
+  static constexpr int PC = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : P0 >= 4 ? 4 : P0 >= 2 ? 2 : 1;
+  static constexpr int PC_EPI = PC >= 2 ? PC / 2 : 1;  // the epilogue also stages E and chi in shared memory
+};
+
+template <int C, int N, int PC_> struct RegC {
+  static constexpr int TPP = RegPlan<N>::TPP;
+  static constexpr int PC = PC_;
+  static constexpr int THREADS = C * PC * TPP;
+  static constexpr int PITCH = N + N / 16;
+  static __device__ __forceinline__ int idx(int c, int row, int m) { return (c * PC + row) * PITCH + m + (m >> 4); }
+};
+
+// bounded wait on an mbarrier phase; returns false if the copy did not complete within the limit
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(addr), "r"(bytes) : "memory");
+}
+
+// one bulk global -> shared copy (16-byte aligned addresses, size a multiple of 16), completing on the mbarrier
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, unsigned bytes, uint64_t* bar) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+               "l"(gsrc), "r"(bytes), "r"(b)
+               : "memory");
+}
+
+// in-place shared-memory stage for the contiguous layout
+template <int DIR, int N, int C, int PC_, int RAD, int L>
+__device__ __forceinline__ void cstage_smem(float2* __restrict__ sm, const float2* __restrict__ tw) {
+  using G = RegC<C, N, PC_>;
+  constexpr int TPP = G::TPP, PC = G::PC;
+  constexpr int T = N / RAD;
+  constexpr int NBT = T / TPP;
+  constexpr int TSTRIDE = N / (L * RAD);
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  float2 u[NBT][RAD];
+#pragma unroll
+  for (int m = 0; m < NBT; ++m) {
+    const int i = ii + m * TPP;
+    const int kk = i % L;
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) u[m][q] = sm[G::idx(c, row, i + q * T)];
+    if constexpr (L > 1) {
+#pragma unroll
+      for (int q = 1; q < RAD; ++q) {
+        float2 w = tw[q * kk * TSTRIDE];
+        if (DIR > 0) w = conjc(w);
+        u[m][q] = u[m][q] * w;
+      }
+    }
+    bfly<float, RAD, DIR>(u[m], tw, N);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < NBT; ++m) {
+    const int i = ii + m * TPP;
+    const int kk = i % L;
+    const int d0 = (i - kk) * RAD + kk;
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, d0 + q * L)] = u[m][q];
+  }
+  __syncthreads();
+}
+
+template <int... Rs> struct RadixInfo;
+template <int R0, int... Rs> struct RadixInfo<R0, Rs...> {
+  static constexpr int first = R0;
+  static constexpr int count = 1 + sizeof...(Rs);
+};
+template <int... Rs> struct LastRadix;
+template <int R0> struct LastRadix<R0> { static constexpr int value = R0; };
+template <int R0, int R1, int... Rs> struct LastRadix<R0, R1, Rs...> {
+  static constexpr int value = LastRadix<R1, Rs...>::value;
+};
+
+// middle stages of a plan (all but first and last), starting at L = first radix
+template <int DIR, int N, int C, int PC, int L, int... Rs> struct CMidOfPlan;
+template <int DIR, int N, int C, int PC, int L, int R0> struct CMidOfPlan<DIR, N, C, PC, L, R0> {
+  static __device__ __forceinline__ void run(float2*, const float2*) {}
+};
+template <int DIR, int N, int C, int PC, int L, int R0, int R1, int... Rs>
+struct CMidOfPlan<DIR, N, C, PC, L, R0, R1, Rs...> {
+  static __device__ __forceinline__ void run(float2* sm, const float2* tw) {
+    cstage_smem<DIR, N, C, PC, R0, L>(sm, tw);
+    CMidOfPlan<DIR, N, C, PC, L * R0, R1, Rs...>::run(sm, tw);
+  }
+};
+
+template <class PL> struct RegPlanArgs;
+template <int... Rs> struct RegPlanArgs<RegPlanList<Rs...>> {
+  static constexpr int R_first = RadixInfo<Rs...>::first;
+  static constexpr int R_last = LastRadix<Rs...>::value;
+  static constexpr int count = RadixInfo<Rs...>::count;
+  template <int DIR, int N, int C, int PC> static __device__ __forceinline__ void mid(float2* sm, const float2* tw) {
+    // stages 2 .. count-1 (skip the first, stop before the last)
+    MidHelper<DIR, N, C, PC, Rs...>::run(sm, tw);
+  }
+  template <int DIR, int N, int C, int PC, int R0, int... Rest> struct MidHelper {
+    static __device__ __forceinline__ void run(float2* sm, const float2* tw) {
+      CMidOfPlan<DIR, N, C, PC, R0, Rest...>::run(sm, tw);
+    }
+  };
+};
+
+template <int C, int OPS, int N, int PC_>
+__global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, 2) k_regc_pass(IterArgs<float> a) {
+  using G = RegC<C, N, PC_>;
+  using PA = RegPlanArgs<typename RegPlan<N>::type>;
+  constexpr int TPP = G::TPP, PC = G::PC, THREADS = G::THREADS;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * PC * G::PITCH;
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  if (!st->active) return;
+  const ChiCoef<float> cc = chi_coef<float>(st);
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int64_t N3 = a.N;
+  const int64_t fbase = (int64_t)b * C * N3;
+  const int64_t rowbase = ((int64_t)blockIdx.x * PC + row) * N;  // voxel index of sample 0 of this row
+  const int cur = st->cur;
+  const float2* __restrict__ Ecur = cur ? a.E1 : a.E0;
+  float2* __restrict__ Eoth = cur ? a.E0 : a.E1;
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  __syncthreads();
+
+  if constexpr (OPS == (OP_PRO | OP_FWD)) {
+    // first stage: x = chi E + s' from global, radix R_first, L = 1, outputs to shared memory
+    constexpr int RAD = PA::R_first;
+    constexpr int T = N / RAD;
+    constexpr int NBT = T / TPP;
+    float2 u[NBT][RAD];
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int i = ii + m * TPP;
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) {
+        const int64_t vox = rowbase + i + q * T;
+        const float2 x = cc.a * a.chi[vox] + cc.b;
+        u[m][q] = x * Ecur[fbase + c * N3 + vox] + cc.s * a.src[fbase + c * N3 + vox];
+      }
+      bfly<float, RAD, -1>(u[m], smtw, N);
+    }
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int i = ii + m * TPP;
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[m][q];
+    }
+    __syncthreads();
+    PA::template mid<-1, N, C, PC>(sm, smtw);
+    // last stage: shared -> registers -> T (global)
+    constexpr int RL = PA::R_last;
+    constexpr int TL = N / RL;
+    constexpr int NBL = TL / TPP;
+    constexpr int LL = N / RL;
+    float2 v[NBL][RL];
+#pragma unroll
+    for (int m = 0; m < NBL; ++m) {
+      const int i = ii + m * TPP;
+#pragma unroll
+      for (int q = 0; q < RL; ++q) v[m][q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+      for (int q = 1; q < RL; ++q) v[m][q] = v[m][q] * smtw[q * i];
+      bfly<float, RL, -1>(v[m], smtw, N);
+#pragma unroll
+      for (int q = 0; q < RL; ++q) a.T[fbase + c * N3 + rowbase + i + q * LL] = v[m][q];
+    }
+  } else {
+    // INV | EPI.  E and chi of the tile's rows are contiguous chunks (PC rows x N samples per component): fetch
+    // them with bulk copies into shared memory now, so they arrive while the inverse transform of T runs.
+    float2* smE = smtw + N;              // [C][PC][N]
+    float2* smX = smE + C * PC * N;      // [PC][N]
+    __shared__ __align__(8) uint64_t bar;
+    const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
+    const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+    if (tid == 0) {
+      mbar_init(&bar, 1);
+      mbar_expect_tx(&bar, chunk * (C + 1));
+#pragma unroll
+      for (int cc2 = 0; cc2 < C; ++cc2) bulk_load(smE + cc2 * PC * N, Ecur + fbase + cc2 * N3 + row0, chunk, &bar);
+      bulk_load(smX, a.chi + row0, chunk, &bar);
+    }
+    // first stage from T (global) into shared memory
+    constexpr int RAD = PA::R_first;
+    constexpr int T = N / RAD;
+    constexpr int NBT = T / TPP;
+    float2 u[NBT][RAD];
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int i = ii + m * TPP;
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) u[m][q] = a.T[fbase + c * N3 + rowbase + i + q * T];
+      bfly<float, RAD, +1>(u[m], smtw, N);
+    }
+#pragma unroll
+    for (int m = 0; m < NBT; ++m) {
+      const int i = ii + m * TPP;
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[m][q];
+    }
+    __syncthreads();
+    PA::template mid<+1, N, C, PC>(sm, smtw);
+    constexpr int RL = PA::R_last;
+    constexpr int TL = N / RL;
+    constexpr int NBL = TL / TPP;
+    constexpr int LL = N / RL;
+    double dd2 = 0.0, en2 = 0.0;
+    const bool staged = mbar_wait(&bar, 0);  // bounded: on a timeout, fall back to global loads
+    const float2* eS = staged ? smE + (c * PC + row) * N : Ecur + fbase + c * N3 + rowbase;
+    const float2* xS = staged ? smX + row * N : a.chi + rowbase;
+    float2 v[NBL][RL];
+#pragma unroll
+    for (int m = 0; m < NBL; ++m) {
+      const int i = ii + m * TPP;
+#pragma unroll
+      for (int q = 0; q < RL; ++q) v[m][q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+      for (int q = 1; q < RL; ++q) v[m][q] = v[m][q] * conjc(smtw[q * i]);
+      bfly<float, RL, +1>(v[m], smtw, N);
+#pragma unroll
+      for (int q = 0; q < RL; ++q) {
+        const int s_ = i + q * LL;
+        const float2 e = eS[s_];
+        const float2 x = cc.a * xS[s_] + cc.b;
+        const float2 d = x * (v[m][q] - e);
+        const float2 en = e + d;
+        Eoth[fbase + c * N3 + rowbase + s_] = en;
+        dd2 += norm2d(d);
+        en2 += norm2d(en);
+      }
+    }
+    if (!staged && tid == 0) {
+      // the bulk copy did not complete in time: flag it and drain it (bounded) before the block exits
+      atomicOr(&const_cast<mmx_rhs_state*>(st)->status, MMX_STATUS_TIMEOUT);
+      mbar_wait(&bar, 0);
+    }
+    finish_pass_norms(a, b, dd2, en2);
+  }
+}

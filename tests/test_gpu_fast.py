@@ -72,3 +72,39 @@ def test_specialised_matches_oracle(name):
             break
     for it in (1, 5, 20):
         assert rel(fields[it], rec_ref[it]) < 1e-5, (it, rel(fields[it], rec_ref[it]))
+
+
+def _solution_env(wl, env):
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return _solution(wl)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256', 'mixed_3d'])
+def test_register_staged_matches_shared_staged(name):
+    """k_reg_pass (strided passes, 16-pencil tiles, global<->register first/last stages) vs k_fast_pass."""
+    wl = _cases()[name]()
+    reg = _solution_env(wl, {'MMX_NO_REG': '0'})
+    shm = _solution_env(wl, {'MMX_NO_REG': '1'})
+    reg.solve(None, rtol=0, maxiter=15)
+    shm.solve(None, rtol=0, maxiter=15)
+    assert rel(reg.E, shm.E) < 2e-6
+
+
+def test_register_staged_512_matches_oracle():
+    from macromax_b200 import workloads
+    from oracle import mmoracle as mo
+    wl = workloads.correlated_slab_2d(n=512, nb_modes=1)
+    wl['source'] = wl['source'][0]
+    sol = _solution(wl)
+    ref = mo.from_workload(wl, np.complex128)
+    rec = ref.solve(rtol=0, maxiter=10, record=(10,))
+    sol.solve(None, rtol=0, maxiter=10)
+    assert rel(sol.E, rec[10]) < 1e-5
