@@ -116,6 +116,23 @@ int mmx_iterate(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kin
                 mmx_rhs_state* state, int niter, void* stream);
 
 /*
+ * mmx_iterate for `niter` iterations as one CUDA graph launch: the pass kernels are captured once per (plan,
+ * buffers, niter) and replayed, which removes the per-kernel launch gaps that dominate small grids.  Same
+ * semantics as mmx_iterate.  The captured graph is released with the plan.
+ */
+int mmx_iterate_graph(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                      mmx_rhs_state* state, int niter, void* stream);
+
+/*
+ * `niter` iterations of n independent problems (plans of possibly different grid shapes, e.g. an uneven batch of
+ * 128^2, 256^2 and 384^2 grids) packed into ONE captured CUDA graph whose branches run concurrently.  Arrays of
+ * length n give each plan's buffers as in mmx_iterate.  The reference solves such problems one after another.
+ */
+int mmx_iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1, const void* const* chi,
+                      const int* chi_kind, const void* const* src, mmx_rhs_state* const* state, int niter,
+                      void* stream);
+
+/*
  * Mixed-precision defect of the FP64 outer loop, for a complex128 plan:
  *   s_out = [s'(alpha) + chi(alpha) x - G(alpha)^{-1} x] alpha_i / alpha0_i      (complex128 in, complex64 out)
  * i.e. the source, normalised to alpha0 like every stored source, for which the plain iteration's fixed point is
@@ -142,6 +159,19 @@ int mmx_adjoint_grad(const void* E, const void* nu, void* grad, int64_t batch, i
  */
 int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int b_broadcast, void* out,
                       int64_t nvox, int precision, void* stream);
+
+/*
+ * Set-up reductions over a 3x3 complex128 matrix field M [9][nvox] (row-major entries), FP64, written to
+ * out_dev[0..1] (device):
+ *   mode 0: out_dev[1] = max over voxels of the largest eigenvalue of (ab I - M)^H (ab I - M), the alpha objective
+ *           sqrt(largest_eigenvalue(...)) of solver.py:392-401 (via mat3_eigh, backend/__init__.py:670-850);
+ *   mode 1: out_dev[0], out_dev[1] = min and max over voxels of the eigenvalues of -0.5i (M - M^H), the gain/loss
+ *           test of solver.py:322-336.
+ * Eigenvalues in closed form (trigonometric solution of the characteristic cubic; like the reference's own cubic
+ * roots, accurate to ~1e-8 relative where the largest eigenvalue is (nearly) double).  Uses the plan's scratch.
+ */
+int mmx_mat3_extremes(mmx_plan* plan, const void* M, int64_t nvox, int mode, double ab, double* out_dev,
+                      void* stream);
 
 /*
  * mmx_fftn without a plan and without any device allocation: the same transform as mmx_fftn (forward unscaled,

@@ -34,7 +34,7 @@ def _to_matrix_field(arr, ndim):
     return arr
 
 
-def prepare_material(grid: Grid, epsilon, bound: Bound | None, wavenumber: float, dtype):
+def prepare_material(grid: Grid, epsilon, bound: Bound | None, wavenumber: float, dtype, device=None):
     """Permittivity (plus an Electric bound's susceptibility) as a matrix field, and its preconditioner."""
     bound = bound if bound is not None else PeriodicBound(grid)
     eps = _to_matrix_field(np.asarray(epsilon, dtype=np.complex128), grid.ndim)
@@ -43,7 +43,8 @@ def prepare_material(grid: Grid, epsilon, bound: Bound | None, wavenumber: float
         if eps.shape[0] > 1:
             chi_b = np.eye(3).reshape(3, 3, *([1] * grid.ndim)) * chi_b
         eps = eps + chi_b
-    pre = pc.prepare(eps, bound.thickness, wavenumber, float(np.finfo(np.dtype(dtype)).eps))
+    pre = pc.prepare(eps, bound.thickness, wavenumber, float(np.finfo(np.dtype(dtype)).eps), device_setup=True,
+                     device=device)
     return pre, bound
 
 
@@ -70,7 +71,7 @@ class BatchSolution:
         if self.ncomp not in (1, 3):
             raise ValueError('sources need 1 or 3 components')
         if preconditioner is None:
-            self.pre, self.bound = prepare_material(grid, epsilon, bound, self.wavenumber, self.dtype)
+            self.pre, self.bound = prepare_material(grid, epsilon, bound, self.wavenumber, self.dtype, device=device)
         else:
             self.pre, self.bound = preconditioner, bound
         if self.pre.chi.shape[0] > 1 and self.ncomp != 3:
@@ -141,3 +142,50 @@ class BatchSolution:
 
     def close(self):
         self.engine.close()
+
+
+class UnevenBatch:
+    """
+    Several batches on grids of different sizes (e.g. 64 x 128^2, 32 x 256^2 and 8 x 384^2 sources) iterated by
+    ONE captured CUDA graph per chunk of iterations (``mmx_iterate_multi``): each member's pass kernels form an
+    independent branch of the graph, so the small grids run concurrently instead of one after another.
+    """
+
+    def __init__(self, members):
+        import ctypes
+        self.members = list(members)
+        n = len(self.members)
+        engines = [m.engine for m in self.members]
+        vp = ctypes.c_void_p
+        self._args = (
+            n,
+            (vp * n)(*[e.plan.handle.value for e in engines]),
+            (vp * n)(*[e.fields[0].data_ptr() for e in engines]),
+            (vp * n)(*[e.fields[1].data_ptr() for e in engines]),
+            (vp * n)(*[e.chi.data_ptr() for e in engines]),
+            (ctypes.c_int * n)(*[e.chi_kind for e in engines]),
+            (vp * n)(*[e.sources.data_ptr() for e in engines]),
+            (vp * n)(*[e.state.data_ptr() for e in engines]),
+        )
+
+    def iterate(self, niter: int):
+        import ctypes
+        import torch
+        s = torch.cuda.current_stream().cuda_stream
+        nat.call('mmx_iterate_multi', *self._args, int(niter), ctypes.c_void_p(s) if s else None)
+
+    def solve(self, rtol: float = 1e-6, maxiter=inf, chunk: int = 8, max_chunk: int = 64) -> 'UnevenBatch':
+        for m in self.members:
+            st = m.engine.read_state()
+            st['iteration'] = 0
+            st['rtol'] = rtol
+            st['maxiter'] = maxiter
+            st['active'] = 1
+            st['status'] = 0
+            m.engine.write_state(st)
+        while True:
+            self.iterate(chunk)
+            if not any(np.any(m.engine.read_state()['active']) for m in self.members):
+                break
+            chunk = min(2 * chunk, max_chunk)
+        return self

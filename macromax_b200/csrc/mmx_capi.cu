@@ -88,6 +88,37 @@ struct mmx_plan {
 
 namespace {
 
+// Captured iteration chunks: one executable graph per (plans, buffers, iteration count).
+struct GraphKey {
+  std::vector<const void*> ptrs;  // plans and buffers
+  std::vector<int> ints;          // chi kinds, iteration count
+  bool operator==(const GraphKey& o) const { return ptrs == o.ptrs && ints == o.ints; }
+};
+struct GraphEntry {
+  GraphKey key;
+  cudaGraphExec_t exec;
+};
+std::mutex g_graph_mutex;
+std::vector<GraphEntry> g_graphs;
+
+void drop_graphs_of(const mmx_plan* p) {
+  std::lock_guard<std::mutex> lock(g_graph_mutex);
+  for (size_t i = 0; i < g_graphs.size();) {
+    bool uses = false;
+    for (const void* q : g_graphs[i].key.ptrs) uses |= (q == (const void*)p);
+    if (uses) {
+      cudaGraphExecDestroy(g_graphs[i].exec);
+      g_graphs.erase(g_graphs.begin() + i);
+    } else {
+      ++i;
+    }
+  }
+}
+
+}  // namespace
+
+namespace {
+
 bool factorize(int n, FFTAxis& ax) {
   ax.n = n;
   ax.nst = 0;
@@ -596,6 +627,7 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
 
 int mmx_plan_destroy(mmx_plan* p) {
   if (!p) return MMX_OK;
+  drop_graphs_of(p);
   for (int i = 0; i < 3; ++i)
     if (p->tw_dev[i]) cudaFree(p->tw_dev[i]);
   if (p->kv_dev) cudaFree(p->kv_dev);
@@ -723,6 +755,111 @@ int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int 
 }
 
 }  // extern "C"
+
+namespace {
+
+// Capture `niter` iterations of every plan into one graph: the plans' passes run on forked capture streams, so
+// independent grids (e.g. batches of uneven sizes) become parallel branches of a single launch.
+int capture_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1, const void* const* chi,
+                  const int* chi_kind, const void* const* src, mmx_rhs_state* const* st, int niter,
+                  cudaGraphExec_t* out) {
+  std::vector<cudaStream_t> streams(n + 1, nullptr);
+  std::vector<cudaEvent_t> events(n + 1, nullptr);
+  int rc = MMX_OK;
+  cudaGraph_t graph = nullptr;
+  bool capturing = false;
+  for (int i = 0; i <= n && rc == MMX_OK; ++i) {
+    if (cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&events[i], cudaEventDisableTiming) != cudaSuccess)
+      rc = fail(MMX_ERR_CUDA, "graph capture: stream/event creation failed");
+  }
+  if (rc == MMX_OK) {
+    cudaError_t e = cudaStreamBeginCapture(streams[0], cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamBeginCapture");
+    else capturing = true;
+  }
+  if (rc == MMX_OK) {
+    cudaEventRecord(events[n], streams[0]);  // fork point
+    for (int i = 0; i < n && rc == MMX_OK; ++i) {
+      cudaStreamWaitEvent(streams[i + 1], events[n], 0);
+      mmx_plan* p = plans[i];
+      if (p->prec == MMX_C128)
+        rc = run_iterations<double>(p, E0[i], E1[i], chi[i], chi_kind[i], src[i], st[i], niter, streams[i + 1]);
+      else
+        rc = run_iterations<float>(p, E0[i], E1[i], chi[i], chi_kind[i], src[i], st[i], niter, streams[i + 1]);
+      cudaEventRecord(events[i], streams[i + 1]);
+      cudaStreamWaitEvent(streams[0], events[i], 0);  // join
+    }
+  }
+  if (capturing) {
+    cudaError_t e = cudaStreamEndCapture(streams[0], &graph);
+    if (rc == MMX_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
+  }
+  if (rc == MMX_OK) {
+    cudaError_t e = cudaGraphInstantiate(out, graph, 0);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate");
+  }
+  if (graph) cudaGraphDestroy(graph);
+  for (int i = 0; i <= n; ++i) {
+    if (events[i]) cudaEventDestroy(events[i]);
+    if (streams[i]) cudaStreamDestroy(streams[i]);
+  }
+  cudaGetLastError();
+  return rc;
+}
+
+}  // namespace
+
+extern "C" int mmx_iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1,
+                                 const void* const* chi, const int* chi_kind, const void* const* src,
+                                 mmx_rhs_state* const* state, int niter, void* stream) {
+  if (n < 1 || !plans || !E0 || !E1 || !chi || !chi_kind || !src || !state) return fail(MMX_ERR_ARG, "NULL argument");
+  if (niter < 1) return fail(MMX_ERR_ARG, "niter must be positive");
+  GraphKey key;
+  for (int i = 0; i < n; ++i) {
+    mmx_plan* p = plans[i];
+    if (!p || !E0[i] || !E1[i] || !chi[i] || !src[i] || !state[i]) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+    if (chi_kind[i] != MMX_CHI_SCALAR && chi_kind[i] != MMX_CHI_MAT3) return fail(MMX_ERR_ARG, "unknown chi_kind");
+    if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
+    key.ptrs.insert(key.ptrs.end(), {(const void*)p, E0[i], E1[i], chi[i], src[i], (const void*)state[i]});
+    key.ints.push_back(chi_kind[i]);
+  }
+  key.ints.push_back(niter);
+  cudaGraphExec_t exec = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_graph_mutex);
+    for (const GraphEntry& g : g_graphs)
+      if (g.key == key) exec = g.exec;
+  }
+  if (!exec) {
+    const int rc = capture_multi(n, plans, E0, E1, chi, chi_kind, src, state, niter, &exec);
+    if (rc != MMX_OK) return rc;
+    std::lock_guard<std::mutex> lock(g_graph_mutex);
+    g_graphs.push_back(GraphEntry{key, exec});
+  }
+  MMX_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
+  return MMX_OK;
+}
+
+extern "C" int mmx_iterate_graph(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                                 mmx_rhs_state* state, int niter, void* stream) {
+  return mmx_iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, stream);
+}
+
+extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,
+                                 void* stream) {
+  if (!p || !M || !out_dev) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (mode != 0 && mode != 1) return fail(MMX_ERR_ARG, "mode must be 0 or 1");
+  if (nvox < 1) return fail(MMX_ERR_ARG, "nvox must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  int blocks = grid_blocks(nvox, 256);
+  if (2 * (int64_t)blocks > p->partials_len) blocks = (int)(p->partials_len / 2);
+  k_mat3_extremes<<<blocks, 256, 0, s>>>((const double2*)M, nvox, mode, ab, p->partials);
+  MMX_CUDA(cudaGetLastError());
+  k_minmax_final<<<1, 256, 0, s>>>(p->partials, blocks, out_dev);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // Allocation-free N-D FFT.

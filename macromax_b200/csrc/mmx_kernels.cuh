@@ -463,3 +463,157 @@ __global__ void k_pointwise_mul(const cpx<R>* __restrict__ A, int ra, int ca, co
       }
   }
 }
+
+// ------------------------------------------------------------------------------------------------------------
+// Set-up reductions over 3x3 permittivity fields (FP64): the largest eigenvalue of (ab I - M)^H (ab I - M) for the
+// alpha objective (solver.py:392-401) and the extreme eigenvalues of the anti-Hermitian part -0.5i (M - M^H) for the
+// gain / loss checks (solver.py:322-336).  Eigenvalues of a Hermitian 3x3 matrix in closed form: trigonometric
+// solution of the characteristic cubic, q = tr/3, p = sqrt(tr((H - qI)^2)/6), r = det((H - qI)/p)/2,
+// lambda_k = q + 2p cos(acos(r)/3 + 2 pi k/3).
+// ------------------------------------------------------------------------------------------------------------
+__device__ __forceinline__ void herm3_extremes(const double h[3][3][2], double* lmin, double* lmax) {
+  // h[i][j] = (re, im), Hermitian: real diagonal, h[j][i] = conj(h[i][j])
+  const double q = (h[0][0][0] + h[1][1][0] + h[2][2][0]) / 3.0;
+  const double p1 = h[0][1][0] * h[0][1][0] + h[0][1][1] * h[0][1][1] + h[0][2][0] * h[0][2][0] +
+                    h[0][2][1] * h[0][2][1] + h[1][2][0] * h[1][2][0] + h[1][2][1] * h[1][2][1];
+  const double d0 = h[0][0][0] - q, d1 = h[1][1][0] - q, d2 = h[2][2][0] - q;
+  const double p2 = d0 * d0 + d1 * d1 + d2 * d2 + 2.0 * p1;
+  if (p2 <= 0.0) {
+    *lmin = q;
+    *lmax = q;
+    return;
+  }
+  const double p = sqrt(p2 / 6.0);
+  const double ip = 1.0 / p;
+  const double b00 = d0 * ip, b11 = d1 * ip, b22 = d2 * ip;
+  const double b01r = h[0][1][0] * ip, b01i = h[0][1][1] * ip;
+  const double b02r = h[0][2][0] * ip, b02i = h[0][2][1] * ip;
+  const double b12r = h[1][2][0] * ip, b12i = h[1][2][1] * ip;
+  // det B = b00 b11 b22 + 2 Re(b01 b12 conj(b02)) - b00 |b12|^2 - b11 |b02|^2 - b22 |b01|^2
+  const double re_t = (b01r * b12r - b01i * b12i) * b02r + (b01r * b12i + b01i * b12r) * b02i;
+  double r = 0.5 * (b00 * b11 * b22 + 2.0 * re_t - b00 * (b12r * b12r + b12i * b12i) -
+                    b11 * (b02r * b02r + b02i * b02i) - b22 * (b01r * b01r + b01i * b01i));
+  r = fmin(1.0, fmax(-1.0, r));
+  const double phi = acos(r) / 3.0;
+  *lmax = q + 2.0 * p * cos(phi);
+  *lmin = q + 2.0 * p * cos(phi + 2.0943951023931954923);  // + 2 pi / 3
+}
+
+// mode 0: out = max_v lambda_max((ab I - M_v)^H (ab I - M_v)); mode 1: out = (min_v, max_v) of the eigenvalues of
+// -0.5i (M_v - M_v^H).  M: [9][N] complex128.  Block partials in part[2 * block].
+__global__ void k_mat3_extremes(const double2* __restrict__ M, int64_t N, int mode, double ab, double* part) {
+  double vmin = INFINITY, vmax = -INFINITY;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (int64_t)gridDim.x * blockDim.x) {
+    double a[3][3][2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double2 z = M[(int64_t)(i * 3 + j) * N + v];
+        a[i][j][0] = z.x;
+        a[i][j][1] = z.y;
+      }
+    double h[3][3][2];
+    if (mode == 0) {
+      // D = ab I - M; H = D^H D
+      double d[3][3][2];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          d[i][j][0] = (i == j ? ab : 0.0) - a[i][j][0];
+          d[i][j][1] = -a[i][j][1];
+        }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          double re = 0.0, im = 0.0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {  // conj(d[k][i]) * d[k][j]
+            re += d[k][i][0] * d[k][j][0] + d[k][i][1] * d[k][j][1];
+            im += d[k][i][0] * d[k][j][1] - d[k][i][1] * d[k][j][0];
+          }
+          h[i][j][0] = re;
+          h[i][j][1] = im;
+        }
+    } else {
+      // -0.5i (M - M^H) (solver.py:324): entry -(i/2)(m_ij - conj(m_ji)); diagonal = Im m_ii
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const double xr = a[i][j][0] - a[j][i][0], xi = a[i][j][1] + a[j][i][1];
+          h[i][j][0] = 0.5 * xi;
+          h[i][j][1] = -0.5 * xr;
+        }
+    }
+    double lo, hi;
+    herm3_extremes(h, &lo, &hi);
+    vmin = fmin(vmin, lo);
+    vmax = fmax(vmax, hi);
+  }
+  // block min / max
+  __shared__ double smin[32], smax[32];
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    vmin = fmin(vmin, __shfl_down_sync(full, vmin, o));
+    vmax = fmax(vmax, __shfl_down_sync(full, vmax, o));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smin[warp] = vmin;
+    smax[warp] = vmax;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    vmin = lane < nw ? smin[lane] : INFINITY;
+    vmax = lane < nw ? smax[lane] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmin = fmin(vmin, __shfl_down_sync(full, vmin, o));
+      vmax = fmax(vmax, __shfl_down_sync(full, vmax, o));
+    }
+    if (lane == 0) {
+      part[2 * blockIdx.x] = vmin;
+      part[2 * blockIdx.x + 1] = vmax;
+    }
+  }
+}
+
+__global__ void k_minmax_final(const double* __restrict__ part, int np, double* out) {
+  double vmin = INFINITY, vmax = -INFINITY;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    vmin = fmin(vmin, part[2 * i]);
+    vmax = fmax(vmax, part[2 * i + 1]);
+  }
+  __shared__ double smin[32], smax[32];
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    vmin = fmin(vmin, __shfl_down_sync(full, vmin, o));
+    vmax = fmax(vmax, __shfl_down_sync(full, vmax, o));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smin[warp] = vmin;
+    smax[warp] = vmax;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    vmin = lane < nw ? smin[lane] : INFINITY;
+    vmax = lane < nw ? smax[lane] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmin = fmin(vmin, __shfl_down_sync(full, vmin, o));
+      vmax = fmax(vmax, __shfl_down_sync(full, vmax, o));
+    }
+    if (lane == 0) {
+      out[0] = vmin;
+      out[1] = vmax;
+    }
+  }
+}

@@ -150,10 +150,13 @@ class IterationEngine:
         self.write_state(st)
 
     # -- iteration --------------------------------------------------------------------------------------------------
+    use_graphs = True  # replay captured CUDA graphs for multi-iteration chunks
+
     def iterate(self, niter: int, stream=None):
         if niter <= 0:
             return
-        nat.call('mmx_iterate', self.plan.handle, _ptr(self.fields[0]), _ptr(self.fields[1]), _ptr(self.chi),
+        fn = 'mmx_iterate_graph' if (self.use_graphs and niter > 1) else 'mmx_iterate'
+        nat.call(fn, self.plan.handle, _ptr(self.fields[0]), _ptr(self.fields[1]), _ptr(self.chi),
                  self.chi_kind, _ptr(self.sources), _ptr(self.state), int(niter), _stream_ptr(stream))
 
     def run(self, rtol: float, maxiter: float, chunk: int = 8, max_chunk: int = 64) -> np.ndarray:

@@ -78,16 +78,65 @@ class Preconditioner:
     eps_field: np.ndarray  # [1|3, 1|3, *shape] complex128
 
 
+class DeviceSetup:
+    """
+    The set-up reductions of an anisotropic (3x3) permittivity on the GPU (``mmx_mat3_extremes``): the alpha
+    objective and the gain / loss test, in FP64 with closed-form 3x3 eigenvalues.  On a 192^3 grid a host
+    ``eigvalsh`` pass takes seconds and Nelder-Mead needs ~30 of them.
+    """
+
+    def __init__(self, eps_field: np.ndarray, device=None):
+        import ctypes
+        import torch
+        from . import _native as nat
+        self._nat, self._ctypes, self._torch = nat, ctypes, torch
+        ndim = eps_field.ndim - 2
+        shape = eps_field.shape[2:]
+        self.nvox = int(np.prod(shape))
+        dev = torch.device(device if device is not None else 'cuda')
+        m = np.ascontiguousarray(np.broadcast_to(eps_field, (3, 3, *shape)).reshape(9, self.nvox), np.complex128)
+        self.M = torch.from_numpy(m).to(dev)
+        self.out = torch.zeros(2, dtype=torch.float64, device=dev)
+        with torch.cuda.device(dev):
+            self.plan = nat.Plan((8,) * max(1, min(ndim, 1)), 1, 1, nat.MMX_C128)
+
+    def _run(self, mode: int, ab: float):
+        c = self._ctypes
+        s = self._torch.cuda.current_stream().cuda_stream
+        self._nat.call('mmx_mat3_extremes', self.plan.handle, c.c_void_p(self.M.data_ptr()), self.nvox, mode,
+                       float(ab), c.c_void_p(self.out.data_ptr()), c.c_void_p(s) if s else None)
+        return self.out.cpu().numpy()
+
+    def sigma(self, alpha_real, beta: float) -> float:
+        ab = float(np.ravel(np.real(alpha_real))[0]) * beta
+        lam = float(self._run(0, ab)[1])
+        return abs(lam) ** 0.5 / abs(beta)
+
+    def gain_loss(self, eps_dtype: float):
+        lo, hi = self._run(1, 0.0)
+        thr = math.sqrt(eps_dtype)
+        return bool(lo < -thr), bool(hi > thr)
+
+
 def prepare(eps_field: np.ndarray, thickness: np.ndarray, wavenumber: float, eps_dtype: float,
-            mu: complex = 1.0, objective=None) -> Preconditioner:
+            mu: complex = 1.0, objective=None, device_setup: bool = False, device=None) -> Preconditioner:
     """
     eps_field: permittivity as a matrix field [1|3, 1|3, *grid] (boundary susceptibility included).
-    objective: optional callable alpha_r -> sigma replacing ``largest_sigma`` (e.g. a device implementation).
+    objective: optional callable alpha_r -> sigma replacing ``largest_sigma``.
+    device_setup: evaluate the anisotropic objective and the gain/loss test on the GPU (DeviceSetup).
     """
     beta = float(np.real(1.0 / mu))  # solver.py:446
-    gain = has_gain(eps_field, eps_dtype)
-    loss = has_gain(-eps_field, eps_dtype)
+    dev = None
+    if device_setup and not _is_scalar_field(eps_field):
+        dev = DeviceSetup(eps_field, device)
+        gain, loss = dev.gain_loss(eps_dtype)
+    else:
+        gain = has_gain(eps_field, eps_dtype)
+        loss = has_gain(-eps_field, eps_dtype)
     transpose = gain and not loss
+    if objective is None and dev is not None:
+        def objective(ar):
+            return dev.sigma(ar, beta)
     if objective is None:
         def objective(ar):
             return largest_sigma(ar, beta, eps_field)

@@ -128,7 +128,8 @@ class Solution:
         if eps_field.shape[0] > 1 and not self._vectorial:
             raise ValueError('an anisotropic permittivity needs a vector source')
         eps_dtype = float(np.finfo(self._dtype).eps)
-        self._pre = pc.prepare(eps_field, self._bound.thickness, self._wavenumber, eps_dtype, mu=self._mu)
+        self._pre = pc.prepare(eps_field, self._bound.thickness, self._wavenumber, eps_dtype, mu=self._mu,
+                               device_setup=True, device=self._device)
         self._eps_field = eps_field
         alpha = self._pre.alpha
         if self._engine is None:
