@@ -185,15 +185,17 @@ def bench_ours(args, wl, rank, world, local, pg):
     nvox = eng.N
     c = eng.ncomp
     m = 1 if eng.chi_kind == nat.MMX_CHI_SCALAR else 9
-    # keep every step a real iteration: disable the stop rule
+    # every step is a real iteration: the stop rule is disabled for the timed run
     st = eng.read_state()
     st['rtol'] = -1.0
     st['maxiter'] = np.inf
     st['active'] = 1
     eng.write_state(st)
     stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
-        eng.iterate(1)
+    chunk = max(1, min(args.chunk, args.steps))
+    nchunks, rem = divmod(args.steps, chunk)
+    eng.iterate(args.warmup) if args.warmup > 1 else eng.iterate(1)  # warm-up steps (one captured graph)
+    eng.prepare_graph(chunk)  # capture the timed chunk's graph outside the timed region
     torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
@@ -201,29 +203,32 @@ def bench_ours(args, wl, rank, world, local, pg):
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
         start.record(stream)
-        eng.iterate(args.steps)
+        for _ in range(nchunks):
+            eng.iterate(chunk)
+        for _ in range(rem):
+            eng.iterate(1)
         stop.record(stream)
         torch.cuda.synchronize()
     if pg is not None:
         pg.barrier()
     ms = start.elapsed_time(stop)
     if pg is not None:
-        t = torch.tensor([ms], device='cuda')
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+        from macromax_b200.distributed import max_over_ranks
+        ms = max_over_ranks(ms, device='cuda')
     ms_per_step = ms / args.steps
     value = world * nvox * args.steps / (ms / 1e3)
     st = eng.read_state()
     assert np.all(st['status'] == 0) and np.all(st['iteration'] >= args.steps), 'iteration did not run'
-    launches_per_iter = len_passes(wl) + 1
-    # roofline over one iteration
+    launches_per_iter = len_passes(wl)
     alg = algorithmic_bytes(nvox, c, m, dtype)
     peaks = load_peaks()
     achieved = alg / (ms_per_step / 1e3) / 1e9
     roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-            'frac': achieved / peaks['hbm_gbs'], 'traffic': None, 'peak_source': peaks['source'],
-            'unit_of_launch': 'one iteration (pass kernels + decide)', 'algorithmic_bytes': alg}
-    # end to end: one full solve through the public API from host arrays
+            'frac': achieved / peaks['hbm_gbs'], 'traffic': traffic_per_iteration(wl),
+            'peak_source': peaks['source'],
+            'unit_of_launch': f'one iteration = {launches_per_iter} pass kernels (CUDA graph chunks of {chunk})',
+            'algorithmic_bytes': alg, 'bytes_per_voxel': alg / nvox}
+    sol._engine.close()
     e2e = e2e_solve(wl, dtype) if rank == 0 and not args.no_e2e else None
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -231,6 +236,7 @@ def bench_ours(args, wl, rank, world, local, pg):
         cpu = {'value': rate, 'unit': UNIT, 'cores': os.cpu_count() or 1, 'kind': 'port',
                'sample': f'{args.cpu_iters} iterations of the numpy oracle on the full workload ({dt:.1f} s), '
                          f'scipy.fft with {os.cpu_count()} workers'}
+    secondary = run_secondary(args) if rank == 0 and args.secondary != 'none' else None
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
@@ -240,8 +246,92 @@ def bench_ours(args, wl, rank, world, local, pg):
             'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clocks.summary(),
             'gpu_launches': launches_per_iter * args.steps,
         }
+        if secondary is not None:
+            line['secondary'] = secondary
         print(json.dumps(line), flush=True)
-    sol._engine.close()
+
+
+def traffic_per_iteration(wl):
+    """DRAM bytes of one iteration from the committed ncu capture of this workload, scaled per voxel (or None)."""
+    path = os.path.join(ROOT, 'profiles', 'traffic.json')
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        key = f"{wl['name']}"
+        if key in d:
+            return float(d[key]['dram_bytes_per_iteration'])
+    except (OSError, ValueError, KeyError):
+        pass
+    return None
+
+
+def run_secondary(args):
+    """
+    The batched forms of the metric on smaller instances of the other configurations (seconds, device-timed by
+    synchronisation around whole solves):
+      - batched mixed precision (2D scalar slab, 512^2 grid, 256 plane-wave sources) to residue 1e-8, against the
+        plain complex64 per-source loop (one Solution per source, to 1e-5: single precision cannot reach 1e-8),
+        measured on 4 sources and scaled to 256;
+      - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve to 1e-6.
+    """
+    import torch
+    from macromax_b200 import Bound, Grid, Solution, adjoint, workloads
+    from macromax_b200.mixed import MixedSolution
+    out = {}
+    wl = workloads.correlated_slab_2d(n=512, nb_modes=256)
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    bound = Bound(grid, thickness=wl['bound_thickness'])
+    t0 = time.perf_counter()
+    ms = MixedSolution(grid, wl['source'], wl['epsilon'], bound=bound, vacuum_wavelength=wl['wavelength'])
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    ms.solve(rtol=1e-8)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    mixed_s = t2 - t1
+    res = float(ms.residues.max())
+    inner = ms.total_inner_iterations
+    ms.close()
+    seq = 0.0
+    its = 0
+    for b in range(4):
+        sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                       source_distribution=wl['source'][b], bound=bound, dtype=np.complex64)
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        sol.solve(None, rtol=1e-5, maxiter=100000)
+        torch.cuda.synchronize()
+        seq += time.perf_counter() - a
+        its += sol.iteration
+        sol._engine.close()
+    plain_256 = seq / 4 * 256
+    out['batched_mixed_slab2d_512x256'] = {
+        'time_to_1e-8_s': mixed_s, 'max_residue': res, 'setup_s': t1 - t0, 'inner_iterations': inner,
+        'plain_c64_loop_to_1e-5_s (4-source sample x 64)': plain_256, 'plain_iterations_per_source': its / 4,
+        'speedup_vs_plain_loop': plain_256 / mixed_s,
+        'voxel_iterations_per_s': 256 * 512 * 512 * inner / mixed_s}
+    wl = workloads.design_3d(n=128, nb_sources=32)
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    k0 = 2 * np.pi / wl['wavelength']
+    eps = torch.tensor(wl['epsilon'], dtype=torch.complex64, device='cuda', requires_grad=True)
+    src = torch.tensor(wl['source'], dtype=torch.complex64, device='cuda')
+    stats = {}
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    E = adjoint.solve(eps, src, grid, k0, bound=Bound(grid, thickness=wl['bound_thickness']), rtol=1e-6,
+                      maxiter=100000, stats=stats)
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    loss = -(E[:, 0][(slice(None),) + wl['patch']].abs() ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    c = time.perf_counter()
+    fi, ai = stats['forward_iterations'], stats['adjoint_iterations']
+    out['adjoint_design3d_128x32'] = {
+        'forward_s': b - a, 'backward_s': c - b, 'forward_iterations_max': int(fi.max()),
+        'adjoint_iterations_max': int(ai.max()),
+        'voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / (c - a)}
+    return out
 
 
 def len_passes(wl) -> int:
@@ -250,6 +340,9 @@ def len_passes(wl) -> int:
 
 
 def e2e_solve(wl, dtype):
+    """One full solve to the workload's residue through the public API from host arrays (host->device copies of
+    chi, source and initial field, device->host copy of the solution).  A first, untimed solve captures the
+    iteration graphs."""
     import torch
     from macromax_b200 import Bound, Grid, Solution
     grid = Grid(shape=wl['shape'], step=wl['step'])
@@ -261,21 +354,26 @@ def e2e_solve(wl, dtype):
     src_host = eng.sources.cpu().numpy()
     e0 = np.zeros((eng.ncomp, *wl['shape']), dtype=dtype)
     pin = [torch.from_numpy(a).pin_memory() for a in (chi_host, src_host, e0)]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    eng.chi.copy_(pin[0], non_blocking=True)
-    eng.sources.copy_(pin[1], non_blocking=True)
-    eng.set_fields(pin[2])
-    st = eng.run(float(wl['rtol']), float(wl['maxiter']))
-    out = eng.current(st)[0].cpu().numpy()
-    dt = time.perf_counter() - t0
-    iters = int(st['iteration'][0])
-    h2d = sum(int(p.numel() * p.element_size()) for p in pin)
-    d2h = int(out.nbytes)
+    result = None
+    for timed in (False, True):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.chi.copy_(pin[0], non_blocking=True)
+        eng.sources.copy_(pin[1], non_blocking=True)
+        eng.set_fields(pin[2])
+        eng.reset_alpha()
+        st = eng.run(float(wl['rtol']), float(wl['maxiter']))
+        out = eng.current(st)[0].cpu().numpy()
+        dt = time.perf_counter() - t0
+        iters = int(st['iteration'][0])
+        h2d = sum(int(p.numel() * p.element_size()) for p in pin)
+        if timed:
+            result = {'value': eng.N * iters / dt, 'unit': UNIT, 'h2d_bytes_per_step': h2d,
+                      'd2h_bytes_per_step': int(out.nbytes), 'iterations': iters, 'seconds': dt,
+                      'residue': float(st['residue'][0]),
+                      'step': f"one solve to residue {wl['rtol']} from host arrays (time to residual)"}
     sol._engine.close()
-    return {'value': eng.N * iters / dt, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
-            'iterations': iters, 'seconds': dt, 'residue': float(st['residue'][0]),
-            'step': f"one solve to residue {wl['rtol']} from host arrays"}
+    return result
 
 
 def load_peaks():
@@ -291,7 +389,7 @@ def load_peaks():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--steps', type=int, default=400)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='spheres3d')
@@ -299,6 +397,8 @@ def main():
     ap.add_argument('--cpu-iters', type=int, default=6)
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--chunk', type=int, default=20, help='iterations per captured CUDA graph in the timed region')
+    ap.add_argument('--secondary', default='batched', choices=['none', 'batched'])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = make_workload(args)

@@ -123,6 +123,10 @@ int mmx_iterate(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kin
 int mmx_iterate_graph(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
                       mmx_rhs_state* state, int niter, void* stream);
 
+/* Capture (and cache) the graph that mmx_iterate_graph would launch, without launching it. */
+int mmx_iterate_graph_prepare(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                              mmx_rhs_state* state, int niter);
+
 /*
  * `niter` iterations of n independent problems (plans of possibly different grid shapes, e.g. an uneven batch of
  * 128^2, 256^2 and 384^2 grids) packed into ONE captured CUDA graph whose branches run concurrently.  Arrays of

@@ -810,9 +810,10 @@ int capture_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E
 
 }  // namespace
 
-extern "C" int mmx_iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1,
-                                 const void* const* chi, const int* chi_kind, const void* const* src,
-                                 mmx_rhs_state* const* state, int niter, void* stream) {
+namespace {
+int iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1, const void* const* chi,
+                  const int* chi_kind, const void* const* src, mmx_rhs_state* const* state, int niter, void* stream,
+                  bool launch) {
   if (n < 1 || !plans || !E0 || !E1 || !chi || !chi_kind || !src || !state) return fail(MMX_ERR_ARG, "NULL argument");
   if (niter < 1) return fail(MMX_ERR_ARG, "niter must be positive");
   GraphKey key;
@@ -837,13 +838,25 @@ extern "C" int mmx_iterate_multi(int n, mmx_plan* const* plans, void* const* E0,
     std::lock_guard<std::mutex> lock(g_graph_mutex);
     g_graphs.push_back(GraphEntry{key, exec});
   }
-  MMX_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
+  if (launch) MMX_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
   return MMX_OK;
+}
+}  // namespace
+
+extern "C" int mmx_iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1,
+                                 const void* const* chi, const int* chi_kind, const void* const* src,
+                                 mmx_rhs_state* const* state, int niter, void* stream) {
+  return iterate_multi(n, plans, E0, E1, chi, chi_kind, src, state, niter, stream, true);
 }
 
 extern "C" int mmx_iterate_graph(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
                                  mmx_rhs_state* state, int niter, void* stream) {
-  return mmx_iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, stream);
+  return iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, stream, true);
+}
+
+extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind,
+                                         const void* src, mmx_rhs_state* state, int niter) {
+  return iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, nullptr, false);
 }
 
 extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,

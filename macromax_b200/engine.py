@@ -159,6 +159,11 @@ class IterationEngine:
         nat.call(fn, self.plan.handle, _ptr(self.fields[0]), _ptr(self.fields[1]), _ptr(self.chi),
                  self.chi_kind, _ptr(self.sources), _ptr(self.state), int(niter), _stream_ptr(stream))
 
+    def prepare_graph(self, niter: int):
+        """Capture the graph of an ``niter``-iteration chunk now (so that a later timed chunk does not)."""
+        nat.call('mmx_iterate_graph_prepare', self.plan.handle, _ptr(self.fields[0]), _ptr(self.fields[1]),
+                 _ptr(self.chi), self.chi_kind, _ptr(self.sources), _ptr(self.state), int(niter))
+
     def run(self, rtol: float, maxiter: float, chunk: int = 8, max_chunk: int = 64) -> np.ndarray:
         """Iterate every active RHS until its stop rule (iteration < maxiter and residue > rtol) fails."""
         st = self.read_state()
