@@ -48,6 +48,7 @@ struct PassCfg {
   int fast = 0;  // 1: compile-time specialised kernel (complex64, N in the specialised set)
   int reg = 0;   // 1: register-staged strided pass (k_reg_pass, 16-pencil tiles)
   int regc = 0;  // 1: register-staged contiguous prologue/epilogue pass (k_regc_pass) for an isotropic chi
+  int pipe = 0;  // 1: persistent double-buffered variant of the same pass (k_pipe_pass)
   int64_t rc_tiles = 0;
   size_t rc_smem = 0;
 };
@@ -80,6 +81,7 @@ struct mmx_plan {
   std::vector<PassCfg> defect_passes;
   bool force_generic = false;  // MMX_FORCE_GENERIC=1: use only the runtime-length kernels (tests)
   bool no_reg = false;         // MMX_NO_REG=1: shared-memory staged kernels for the strided passes (tests)
+  bool pipe = false;           // MMX_PIPE=1: persistent double-buffered prologue/epilogue passes
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
   size_t l2_window = 0;
@@ -299,8 +301,54 @@ int launch_regc(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   }
 }
 
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+template <int C, int OPS, int N>
+int launch_pipe(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  if constexpr (N == 192 || N == 384 || (C == 3 && N > 128)) {
+    return fail(MMX_ERR_ARG, "internal: no persistent kernel for this length");
+  } else {
+    constexpr int PCK = RegCDefault<C, N>::PC_EPI;
+    auto kern = k_pipe_pass<C, OPS, N, PCK>;
+    const size_t smem = PipeLayout<C, OPS, N, PCK>::bytes();
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured_mask & (1 << dev))) {
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+      configured_mask |= (1 << dev);
+    }
+    const int64_t tiles_per_rhs = pc.outer / PCK;
+    const int64_t ntiles = tiles_per_rhs * batch;
+    int blocks_per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, RegC<C, N, PCK>::THREADS, smem);
+    if (blocks_per_sm < 1) blocks_per_sm = 1;
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)sm_count() * blocks_per_sm);
+    a.nrhs = batch;
+    kern<<<(unsigned)grid, RegC<C, N, PCK>::THREADS, smem, s>>>(a, (int)tiles_per_rhs);
+    MMX_CUDA(cudaGetLastError());
+    return MMX_OK;
+  }
+}
+
 template <int C, int CHI, int N>
 int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_t s) {
+  if (pc.pipe && CHI == MMX_CHI_SCALAR) {
+    switch (pc.ops) {
+      case OP_PRO | OP_FWD: return launch_pipe<C, OP_PRO | OP_FWD, N>(pc, a, batch, s);
+      case OP_INV | OP_EPI: return launch_pipe<C, OP_INV | OP_EPI, N>(pc, a, batch, s);
+      default: break;
+    }
+  }
   if (pc.regc && CHI == MMX_CHI_SCALAR) {
     switch (pc.ops) {
       case OP_PRO | OP_FWD: return launch_regc<C, OP_PRO | OP_FWD, N>(pc, a, batch, s);
@@ -396,6 +444,16 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
           case 64 * 4 + 3: pcr = epi ? RegCDefault<3, 64>::PC_EPI : RegCDefault<3, 64>::PC; break;
           case 128 * 4 + 3: pcr = epi ? RegCDefault<3, 128>::PC_EPI : RegCDefault<3, 128>::PC; break;
         }
+        int pcp = 1;
+        switch (n * 4 + p->ncomp) {
+          case 64 * 4 + 1: pcp = RegCDefault<1, 64>::PC_EPI; break;
+          case 128 * 4 + 1: pcp = RegCDefault<1, 128>::PC_EPI; break;
+          case 256 * 4 + 1: pcp = RegCDefault<1, 256>::PC_EPI; break;
+          case 512 * 4 + 1: pcp = RegCDefault<1, 512>::PC_EPI; break;
+          case 64 * 4 + 3: pcp = RegCDefault<3, 64>::PC_EPI; break;
+          case 128 * 4 + 3: pcp = RegCDefault<3, 128>::PC_EPI; break;
+        }
+        if (outer % pcp == 0 && p->pipe) pc.pipe = 1;
         if (outer % pcr == 0) {
           pc.regc = 1;
           pc.rc_tiles = outer / pcr;
@@ -586,6 +644,8 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
     p->force_generic = fg && fg[0] == '1';
     const char* nr = getenv("MMX_NO_REG");
     p->no_reg = nr && nr[0] == '1';
+    const char* pp = getenv("MMX_PIPE");
+    p->pipe = pp && pp[0] == '1';
     const char* lp = getenv("MMX_L2_PERSIST");
     if (lp && lp[0] == '1' && precision == MMX_C64) {
       int maxp = 0, maxw = 0;

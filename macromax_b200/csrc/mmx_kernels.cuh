@@ -44,6 +44,7 @@ template <class R> struct IterArgs {
   R inv_total;           // 1 / N
   float2* aux;           // defect output [B][C][N] complex64
   size_t l2_window;      // bytes of T kept L2-resident (0: off); host-side launch attribute only
+  int nrhs;              // number of right-hand sides (persistent passes)
 };
 
 // |z|^2 accumulated in FP64 (the squares of complex64 words are exact in double)

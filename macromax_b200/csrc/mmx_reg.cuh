@@ -206,7 +206,7 @@ template <int C, int N, int PC_> struct RegC {
 // bounded wait on an mbarrier phase; returns false if the copy did not complete within the limit
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
+  for (int it = 0; it < (1 << 20); ++it) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -459,5 +459,234 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, 2) k_regc_pass(IterA
       mbar_wait(&bar, 0);
     }
     finish_pass_norms(a, b, dd2, en2);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Persistent, double-buffered variants of the contiguous prologue / epilogue passes.
+//
+// Each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ... of all right-hand sides.  The inputs of a tile
+// (PRO: E, chi, s'; EPI: T, E, chi -- PC rows of N contiguous samples per component) arrive by bulk copies, one per
+// row, into shared rows of pitch N + 8 words (the 64-byte skew keeps the 4-rows-per-warp reads conflict-free),
+// completing on the stage's mbarrier.  While a tile is transformed, the copies of the CTA's next-but-one tile are
+// already in flight in the other stage, so DRAM traffic does not stop during the arithmetic.  Waits are bounded:
+// on a timeout the tile is computed from global memory instead and MMX_STATUS_TIMEOUT is raised.
+// ---------------------------------------------------------------------------------------------------------------
+template <int C, int OPS, int N, int PC> struct PipeLayout {
+  static constexpr int RP = N + 8;                                  // staged row pitch (words)
+  static constexpr int NIN = (OPS & OP_PRO) ? (2 * C + 1) : (2 * C + 1);  // PRO: E, s', chi; EPI: T, E, chi
+  static constexpr int STAGE = NIN * PC * RP;                       // words per stage
+  static constexpr int WORK = C * PC * RegC<C, N, PC>::PITCH;
+  static constexpr size_t bytes() { return (size_t)(WORK + N + 2 * STAGE) * sizeof(float2); }
+};
+
+template <int C, int OPS, int N, int PC>
+__global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, 1) k_pipe_pass(IterArgs<float> a, int tiles_per_rhs) {
+  using G = RegC<C, N, PC>;
+  using L = PipeLayout<C, OPS, N, PC>;
+  using PA = RegPlanArgs<typename RegPlan<N>::type>;
+  constexpr int TPP = G::TPP, THREADS = G::THREADS, RP = L::RP;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + L::WORK;
+  float2* stage0 = smtw + N;
+  __shared__ __align__(8) uint64_t bars[2];
+  __shared__ int s_active[2], s_cur[2];
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int64_t N3 = a.N;
+  const int nrhs = a.nrhs;
+  const int64_t ntiles = (int64_t)tiles_per_rhs * nrhs;
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  const unsigned rowbytes = (unsigned)(N * sizeof(float2));
+
+  // input k of a tile (PRO: 0..C-1 = E_c, C..2C-1 = s'_c, 2C = chi; EPI: 0..C-1 = T_c, C..2C-1 = E_c, 2C = chi)
+  auto issue = [&](int s, int64_t t) {
+    const int b = (int)(t / tiles_per_rhs);
+    const int64_t row0 = (t % tiles_per_rhs) * PC;
+    const mmx_rhs_state* st = a.st + b;
+    const int active = st->active;
+    s_active[s] = active;
+    s_cur[s] = st->cur;
+    if (!active) {  // keep the stage's mbarrier phases in step with the tile sequence: complete this phase now
+      mbar_expect_tx(&bars[s], 0u);
+      return;
+    }
+    const float2* Ecur = st->cur ? a.E1 : a.E0;
+    const int64_t fbase = (int64_t)b * C * N3;
+    float2* dst = stage0 + s * L::STAGE;
+    mbar_expect_tx(&bars[s], rowbytes * (unsigned)(L::NIN * PC));
+    for (int k = 0; k < L::NIN; ++k) {
+      const float2* src;
+      if ((OPS & OP_PRO) != 0) src = k < C ? Ecur + fbase + k * N3 : (k < 2 * C ? a.src + fbase + (k - C) * N3 : a.chi);
+      else src = k < C ? a.T + fbase + k * N3 : (k < 2 * C ? Ecur + fbase + (k - C) * N3 : a.chi);
+      for (int r = 0; r < PC; ++r) bulk_load(dst + (k * PC + r) * RP, src + (row0 + r) * N, rowbytes, &bars[s]);
+    }
+  };
+
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    if ((int64_t)blockIdx.x < ntiles) issue(0, blockIdx.x);
+    if ((int64_t)blockIdx.x + gridDim.x < ntiles) issue(1, blockIdx.x + gridDim.x);
+  }
+  __syncthreads();
+
+  int kk = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++kk) {
+    const int s = kk & 1;
+    const unsigned parity = (unsigned)((kk >> 1) & 1);
+    const int b = (int)(t / tiles_per_rhs);
+    const int64_t rowbase = ((t % tiles_per_rhs) * PC + row) * N;
+    const mmx_rhs_state* st = a.st + b;
+    const int64_t fbase = (int64_t)b * C * N3;
+    if (s_active[s]) {
+      const ChiCoef<float> cc = chi_coef<float>(st);
+      const int cur = s_cur[s];
+      const float2* Ecur = cur ? a.E1 : a.E0;
+      float2* Eoth = cur ? a.E0 : a.E1;
+      const bool staged = mbar_wait(&bars[s], parity);
+      if (!staged && tid == 0) atomicOr(&const_cast<mmx_rhs_state*>(st)->status, MMX_STATUS_TIMEOUT);
+      const float2* stg = stage0 + s * L::STAGE;
+      if constexpr ((OPS & OP_PRO) != 0) {
+        constexpr int RAD = PA::R_first;
+        constexpr int T = N / RAD;
+        constexpr int NBT = T / TPP;
+        float2 u[NBT][RAD];
+#pragma unroll
+        for (int m = 0; m < NBT; ++m) {
+          const int i = ii + m * TPP;
+#pragma unroll
+          for (int q = 0; q < RAD; ++q) {
+            const int smp = i + q * T;
+            float2 e, sv, xv;
+            if (staged) {
+              e = stg[(c * PC + row) * RP + smp];
+              sv = stg[((C + c) * PC + row) * RP + smp];
+              xv = stg[(2 * C * PC + row) * RP + smp];
+            } else {
+              e = Ecur[fbase + c * N3 + rowbase + smp];
+              sv = a.src[fbase + c * N3 + rowbase + smp];
+              xv = a.chi[rowbase + smp];
+            }
+            u[m][q] = (cc.a * xv + cc.b) * e + cc.s * sv;
+          }
+          bfly<float, RAD, -1>(u[m], smtw, N);
+        }
+#pragma unroll
+        for (int m = 0; m < NBT; ++m) {
+          const int i = ii + m * TPP;
+#pragma unroll
+          for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[m][q];
+        }
+        __syncthreads();
+        PA::template mid<-1, N, C, PC>(sm, smtw);
+        constexpr int RL = PA::R_last;
+        constexpr int TL = N / RL;
+        constexpr int NBL = TL / TPP;
+        constexpr int LL = N / RL;
+        float2 v[NBL][RL];
+#pragma unroll
+        for (int m = 0; m < NBL; ++m) {
+          const int i = ii + m * TPP;
+#pragma unroll
+          for (int q = 0; q < RL; ++q) v[m][q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+          for (int q = 1; q < RL; ++q) v[m][q] = v[m][q] * smtw[q * i];
+          bfly<float, RL, -1>(v[m], smtw, N);
+#pragma unroll
+          for (int q = 0; q < RL; ++q) a.T[fbase + c * N3 + rowbase + i + q * LL] = v[m][q];
+        }
+        __syncthreads();  // stage buffer and work area free for reuse
+      } else {
+        constexpr int RAD = PA::R_first;
+        constexpr int T = N / RAD;
+        constexpr int NBT = T / TPP;
+        float2 u[NBT][RAD];
+#pragma unroll
+        for (int m = 0; m < NBT; ++m) {
+          const int i = ii + m * TPP;
+#pragma unroll
+          for (int q = 0; q < RAD; ++q) {
+            const int smp = i + q * T;
+            u[m][q] = staged ? stg[(c * PC + row) * RP + smp] : a.T[fbase + c * N3 + rowbase + smp];
+          }
+          bfly<float, RAD, +1>(u[m], smtw, N);
+        }
+#pragma unroll
+        for (int m = 0; m < NBT; ++m) {
+          const int i = ii + m * TPP;
+#pragma unroll
+          for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[m][q];
+        }
+        __syncthreads();
+        PA::template mid<+1, N, C, PC>(sm, smtw);
+        constexpr int RL = PA::R_last;
+        constexpr int TL = N / RL;
+        constexpr int NBL = TL / TPP;
+        constexpr int LL = N / RL;
+        double dd2 = 0.0, en2 = 0.0;
+        float2 v[NBL][RL];
+#pragma unroll
+        for (int m = 0; m < NBL; ++m) {
+          const int i = ii + m * TPP;
+#pragma unroll
+          for (int q = 0; q < RL; ++q) v[m][q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+          for (int q = 1; q < RL; ++q) v[m][q] = v[m][q] * conjc(smtw[q * i]);
+          bfly<float, RL, +1>(v[m], smtw, N);
+#pragma unroll
+          for (int q = 0; q < RL; ++q) {
+            const int smp = i + q * LL;
+            float2 e, xv;
+            if (staged) {
+              e = stg[((C + c) * PC + row) * RP + smp];
+              xv = stg[(2 * C * PC + row) * RP + smp];
+            } else {
+              e = Ecur[fbase + c * N3 + rowbase + smp];
+              xv = a.chi[rowbase + smp];
+            }
+            const float2 d = (cc.a * xv + cc.b) * (v[m][q] - e);
+            const float2 en = e + d;
+            Eoth[fbase + c * N3 + rowbase + smp] = en;
+            dd2 += norm2d(d);
+            en2 += norm2d(en);
+          }
+        }
+        // per-tile partial norms and the fused decision (the block-wide reduction synchronises the block)
+        {
+          __shared__ int s_last;
+          double out2[2];
+          block_reduce_2<float>(dd2, en2, out2);
+          if (tid == 0) {
+            double* dst = a.partials + ((int64_t)b * tiles_per_rhs + (t % tiles_per_rhs)) * 2;
+            dst[0] = out2[0];
+            dst[1] = out2[1];
+            __threadfence();
+            const unsigned prev = atomicAdd(a.done + b, 1u);
+            s_last = (prev == (unsigned)tiles_per_rhs - 1);
+          }
+          __syncthreads();
+          if (s_last) {
+            __threadfence();
+            decide_rhs(const_cast<mmx_rhs_state*>(st), a.partials + (int64_t)b * tiles_per_rhs * 2, tiles_per_rhs);
+            if (tid == 0) a.done[b] = 0u;
+          }
+          __syncthreads();
+        }
+      }
+      if (!staged && tid == 0) mbar_wait(&bars[s], parity);  // drain before the stage is re-armed
+    } else if (tid == 0) {
+      mbar_wait(&bars[s], parity);  // the phase was completed without copies
+    }
+    // refill this stage with the tile two steps ahead
+    if (tid == 0) {
+      const int64_t nxt = t + 2 * (int64_t)gridDim.x;
+      if (nxt < ntiles) issue(s, nxt);
+    }
+    __syncthreads();
   }
 }

@@ -108,3 +108,16 @@ def test_register_staged_512_matches_oracle():
     rec = ref.solve(rtol=0, maxiter=10, record=(10,))
     sol.solve(None, rtol=0, maxiter=10)
     assert rel(sol.E, rec[10]) < 1e-5
+
+
+@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256', 'disks2d_128'])
+def test_persistent_pipeline_matches_single_tile_passes(name):
+    """k_pipe_pass (persistent, double-buffered bulk copies) vs k_regc_pass, bit for bit."""
+    wl = _cases()[name]()
+    pipe = _solution_env(wl, {'MMX_PIPE': '1'})
+    single = _solution_env(wl, {'MMX_PIPE': '0'})
+    pipe.solve(None, rtol=0, maxiter=12)
+    single.solve(None, rtol=0, maxiter=12)
+    assert np.array_equal(pipe.E, single.E)
+    st = pipe._engine.read_state()
+    assert int(st['status'][0]) == 0
