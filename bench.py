@@ -185,6 +185,10 @@ def bench_ours(args, wl, rank, world, local, pg):
     nvox = eng.N
     c = eng.ncomp
     m = 1 if eng.chi_kind == nat.MMX_CHI_SCALAR else 9
+    tuned = None
+    if args.autotune:
+        from macromax_b200 import autotune
+        tuned = autotune.tune(eng, iters=10, use_cache=False)
     # every step is a real iteration: the stop rule is disabled for the timed run
     st = eng.read_state()
     st['rtol'] = -1.0
@@ -245,6 +249,7 @@ def bench_ours(args, wl, rank, world, local, pg):
             'config': {**config_of(args, wl), 'parallelism': f'replicas x{world}'},
             'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clocks.summary(),
             'gpu_launches': launches_per_iter * args.steps,
+            'kernel_variant': tuned,
         }
         if secondary is not None:
             line['secondary'] = secondary
@@ -399,6 +404,7 @@ def main():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--chunk', type=int, default=20, help='iterations per captured CUDA graph in the timed region')
     ap.add_argument('--secondary', default='batched', choices=['none', 'batched'])
+    ap.add_argument('--autotune', type=int, default=1, help='time the kernel variants first and use the fastest')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = make_workload(args)

@@ -164,6 +164,16 @@ int mmx_adjoint_grad(const void* E, const void* nu, void* grad, int64_t batch, i
 int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int b_broadcast, void* out,
                       int64_t nvox, int precision, void* stream);
 
+/* Kernel variants of a plan (bit flags), chosen by the autotuner (macromax_b200/autotune.py). */
+#define MMX_VARIANT_GENERIC 1u        /* runtime-length shared-memory kernels only */
+#define MMX_VARIANT_SHARED_STAGED 2u  /* compile-time kernels without the register-staged passes */
+#define MMX_VARIANT_PERSISTENT 4u     /* persistent double-buffered prologue/epilogue passes */
+
+/* Select the kernel variant of a plan (rebuilds its pass list, drops its captured graphs).  No reference
+ * counterpart: the reference has one implementation per backend. */
+int mmx_plan_set_variant(mmx_plan* plan, unsigned flags);
+unsigned mmx_plan_get_variant(const mmx_plan* plan);
+
 /*
  * Set-up reductions over a 3x3 complex128 matrix field M [9][nvox] (row-major entries), FP64, written to
  * out_dev[0..1] (device):

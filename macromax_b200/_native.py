@@ -24,6 +24,9 @@ MMX_CHI_MAT3 = 9
 MMX_STATUS_OK = 0
 MMX_STATUS_ZERODIV = 1
 MMX_STATUS_TIMEOUT = 2
+MMX_VARIANT_GENERIC = 1
+MMX_VARIANT_SHARED_STAGED = 2
+MMX_VARIANT_PERSISTENT = 4
 
 # numpy mirror of struct mmx_rhs_state (include/macromax_b200.h)
 STATE_DTYPE = np.dtype([
@@ -38,7 +41,7 @@ assert STATE_DTYPE.itemsize == 112
 EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destroy', 'mmx_plan_set_kvectors',
             'mmx_fftn', 'mmx_norm', 'mmx_iterate', 'mmx_defect', 'mmx_accumulate', 'mmx_adjoint_grad',
             'mmx_pointwise_mul', 'mmx_fftn_noalloc', 'mmx_mat3_extremes', 'mmx_iterate_graph',
-            'mmx_iterate_multi', 'mmx_iterate_graph_prepare']
+            'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant']
 
 _lib = None
 
@@ -77,6 +80,8 @@ def load(path: str | None = None):
         'mmx_mat3_extremes': (i32, [vp, vp, i64, i32, dbl, vp, vp]),
         'mmx_iterate_graph': (i32, [vp, vp, vp, vp, i32, vp, vp, i32, vp]),
         'mmx_iterate_graph_prepare': (i32, [vp, vp, vp, vp, i32, vp, vp, i32]),
+        'mmx_plan_set_variant': (i32, [vp, ctypes.c_uint]),
+        'mmx_plan_get_variant': (ctypes.c_uint, [vp]),
         'mmx_iterate_multi': (i32, [i32, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
                                     ctypes.POINTER(vp), ctypes.POINTER(i32), ctypes.POINTER(vp),
                                     ctypes.POINTER(vp), i32, vp]),

@@ -665,8 +665,8 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
   }
   p->iter_passes = build_passes(p, false);
   p->defect_passes = build_passes(p, true);
-  int64_t maxt = 2048;
-  for (auto& pc : p->iter_passes) maxt = std::max<int64_t>(maxt, pc.tiles);
+  int64_t maxt = 2048;  // enough partial sums for any tile width (at most one tile per pencil)
+  for (int i = 0; i < ndim; ++i) maxt = std::max<int64_t>(maxt, p->N / shape[i]);
   p->partials_len = (int64_t)batch * maxt * 2;
   e = cudaMalloc(&p->partials, sizeof(double) * p->partials_len);
   if (e == cudaSuccess) e = cudaMalloc(&p->done, sizeof(unsigned int) * batch);
@@ -917,6 +917,26 @@ extern "C" int mmx_iterate_graph(mmx_plan* p, void* E0, void* E1, const void* ch
 extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind,
                                          const void* src, mmx_rhs_state* state, int niter) {
   return iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, nullptr, false);
+}
+
+extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
+  if (!p) return fail(MMX_ERR_ARG, "NULL plan");
+  if (flags & ~7u) return fail(MMX_ERR_ARG, "unknown variant flags");
+  drop_graphs_of(p);  // captured graphs hold the previous kernels
+  p->force_generic = (flags & MMX_VARIANT_GENERIC) != 0;
+  p->no_reg = (flags & MMX_VARIANT_SHARED_STAGED) != 0;
+  p->pipe = (flags & MMX_VARIANT_PERSISTENT) != 0;
+  p->iter_passes = build_passes(p, false);
+  p->defect_passes = build_passes(p, true);
+  for (auto& pc : p->iter_passes)
+    if (2 * (int64_t)p->batch * pc.tiles > p->partials_len) return fail(MMX_ERR_ARG, "internal: partials too small");
+  return MMX_OK;
+}
+
+extern "C" unsigned mmx_plan_get_variant(const mmx_plan* p) {
+  if (!p) return 0u;
+  return (p->force_generic ? MMX_VARIANT_GENERIC : 0u) | (p->no_reg ? MMX_VARIANT_SHARED_STAGED : 0u) |
+         (p->pipe ? MMX_VARIANT_PERSISTENT : 0u);
 }
 
 extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,
