@@ -186,7 +186,11 @@ def bench_ours(args, wl, rank, world, local, pg):
     c = eng.ncomp
     m = 1 if eng.chi_kind == nat.MMX_CHI_SCALAR else 9
     tuned = None
-    if args.autotune:
+    if args.variant >= 0:
+        from macromax_b200 import autotune
+        autotune.set_variant(eng, args.variant)
+        tuned = {'variant': args.variant, 'pinned': True}
+    elif args.autotune:
         from macromax_b200 import autotune
         tuned = autotune.tune(eng, iters=10, use_cache=False)
     # every step is a real iteration: the stop rule is disabled for the timed run
@@ -223,7 +227,7 @@ def bench_ours(args, wl, rank, world, local, pg):
     value = world * nvox * args.steps / (ms / 1e3)
     st = eng.read_state()
     assert np.all(st['status'] == 0) and np.all(st['iteration'] >= args.steps), 'iteration did not run'
-    launches_per_iter = len_passes(wl)
+    launches_per_iter = len_passes(wl, tuned['variant'] if tuned else 0)
     alg = algorithmic_bytes(nvox, c, m, dtype)
     peaks = load_peaks()
     achieved = alg / (ms_per_step / 1e3) / 1e9
@@ -339,8 +343,12 @@ def run_secondary(args):
     return out
 
 
-def len_passes(wl) -> int:
+def len_passes(wl, variant=0) -> int:
+    """Pass kernels per iteration: one per axis and direction, or 3 for a 3D grid on the plane passes."""
     d = len(wl['shape'])
+    iso = np.asarray(wl['epsilon']).ndim == d
+    if d == 3 and (variant or 0) & 8 and tuple(wl['shape'][1:]) == (128, 128) and iso:
+        return 3
     return 1 if d == 1 else 2 * d - 1
 
 
@@ -405,6 +413,8 @@ def main():
     ap.add_argument('--chunk', type=int, default=20, help='iterations per captured CUDA graph in the timed region')
     ap.add_argument('--secondary', default='batched', choices=['none', 'batched'])
     ap.add_argument('--autotune', type=int, default=1, help='time the kernel variants first and use the fastest')
+    ap.add_argument('--variant', type=int, default=-1,
+                    help='pin the kernel variant (MMX_VARIANT_* flags) instead of autotuning')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     wl = make_workload(args)

@@ -12,6 +12,7 @@
 
 #include "mmx_fast.cuh"
 #include "mmx_reg.cuh"
+#include "mmx_plane.cuh"
 
 #define MMX_ABI_VERSION 1
 
@@ -49,6 +50,7 @@ struct PassCfg {
   int reg = 0;   // 1: register-staged strided pass (k_reg_pass, 16-pencil tiles)
   int regc = 0;  // 1: register-staged contiguous prologue/epilogue pass (k_regc_pass) for an isotropic chi
   int pipe = 0;  // 1: persistent double-buffered variant of the same pass (k_pipe_pass)
+  int plane = 0; // 1: plane pass over the two inner axes of a 3D grid (k_plane_pass), 2-CTA clusters
   int64_t rc_tiles = 0;
   size_t rc_smem = 0;
 };
@@ -82,6 +84,8 @@ struct mmx_plan {
   bool force_generic = false;  // MMX_FORCE_GENERIC=1: use only the runtime-length kernels (tests)
   bool no_reg = false;         // MMX_NO_REG=1: shared-memory staged kernels for the strided passes (tests)
   bool pipe = false;           // MMX_PIPE=1: persistent double-buffered prologue/epilogue passes
+  bool plane = false;          // plane passes over the two inner axes (3D, 128 x 128 planes, isotropic chi)
+  std::vector<PassCfg> plane_passes;  // the 3-pass schedule used when `plane` is set and chi is isotropic
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
   size_t l2_window = 0;
@@ -340,8 +344,37 @@ int launch_pipe(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   }
 }
 
+template <int C, int OPS>
+int launch_plane(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  auto kern = k_plane_pass<C, OPS>;
+  const size_t smem = mmx_plane::smem_bytes();
+  static int configured_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured_mask & (1 << dev))) {
+    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured_mask |= (1 << dev);
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  dim3 grid((unsigned)pc.tiles, (unsigned)batch);  // tiles = 2 n0 C (two CTAs per component plane)
+  kern<<<grid, mmx_plane::THREADS, smem, s>>>(a);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
 template <int C, int CHI, int N>
 int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_t s) {
+  if (pc.plane) {
+    if constexpr (CHI == MMX_CHI_SCALAR && N == mmx_plane::N) {
+      switch (pc.ops) {
+        case OP_PRO | OP_FWD: return launch_plane<C, OP_PRO | OP_FWD>(pc, a, batch, s);
+        case OP_INV | OP_EPI: return launch_plane<C, OP_INV | OP_EPI>(pc, a, batch, s);
+        default: break;
+      }
+    }
+    return fail(MMX_ERR_ARG, "internal: plane pass without a plane kernel");
+  }
   if (pc.pipe && CHI == MMX_CHI_SCALAR) {
     switch (pc.ops) {
       case OP_PRO | OP_FWD: return launch_pipe<C, OP_PRO | OP_FWD, N>(pc, a, batch, s);
@@ -486,6 +519,31 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
   return v;
 }
 
+// The 3-pass schedule [PRO FWD ax2 FWD ax1] [FWD G INV ax0] [INV ax1 INV ax2 EPI] of a 3D complex64 grid with
+// 128 x 128 planes (empty when the grid does not qualify).  The axis-0 pass is the one of the 5-pass schedule.
+std::vector<PassCfg> build_plane_passes(const mmx_plan* p) {
+  std::vector<PassCfg> v;
+  if (p->ndim != 3 || p->prec != MMX_C64 || p->force_generic || p->shape[1] != mmx_plane::N ||
+      p->shape[2] != mmx_plane::N)
+    return v;
+  const std::vector<PassCfg> five = build_passes(p, false);
+  if (five.size() != 5 || !five[2].fast) return v;
+  PassCfg pro = five[0];
+  pro.plane = 1;
+  pro.regc = pro.pipe = pro.reg = 0;
+  pro.fast = 1;
+  pro.tiles = 2 * p->shape[0] * p->ncomp;
+  PassCfg epi = five[4];
+  epi.plane = 1;
+  epi.regc = epi.pipe = epi.reg = 0;
+  epi.fast = 1;
+  epi.tiles = pro.tiles;
+  v.push_back(pro);
+  v.push_back(five[2]);
+  v.push_back(epi);
+  return v;
+}
+
 template <class R> IterArgs<R> base_args(mmx_plan* p) {
   IterArgs<R> a;
   memset(&a, 0, sizeof(a));
@@ -513,8 +571,11 @@ int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kin
   a.src = (const cpx<R>*)src;
   a.st = st;
   // the accept/reject decision is taken by the last tile of the epilogue pass (no separate launch)
+  const bool plane = std::is_same<R, float>::value && p->plane && chi_kind == MMX_CHI_SCALAR &&
+                     !p->plane_passes.empty();
+  const std::vector<PassCfg>& passes = plane ? p->plane_passes : p->iter_passes;
   for (int it = 0; it < niter; ++it) {
-    for (const PassCfg& pc : p->iter_passes) {
+    for (const PassCfg& pc : passes) {
       a.ax = p->ax[pc.axis];
       int rc = dispatch_pass<R>(pc, a, p->ncomp, chi_kind, p->batch, s);
       if (rc != MMX_OK) return rc;
@@ -665,6 +726,7 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
   }
   p->iter_passes = build_passes(p, false);
   p->defect_passes = build_passes(p, true);
+  p->plane_passes = build_plane_passes(p);
   int64_t maxt = 2048;  // enough partial sums for any tile width (at most one tile per pencil)
   for (int i = 0; i < ndim; ++i) maxt = std::max<int64_t>(maxt, p->N / shape[i]);
   p->partials_len = (int64_t)batch * maxt * 2;
@@ -921,22 +983,25 @@ extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const 
 
 extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
   if (!p) return fail(MMX_ERR_ARG, "NULL plan");
-  if (flags & ~7u) return fail(MMX_ERR_ARG, "unknown variant flags");
+  if (flags & ~15u) return fail(MMX_ERR_ARG, "unknown variant flags");
   drop_graphs_of(p);  // captured graphs hold the previous kernels
   p->force_generic = (flags & MMX_VARIANT_GENERIC) != 0;
   p->no_reg = (flags & MMX_VARIANT_SHARED_STAGED) != 0;
   p->pipe = (flags & MMX_VARIANT_PERSISTENT) != 0;
+  p->plane = (flags & MMX_VARIANT_PLANE) != 0;
   p->iter_passes = build_passes(p, false);
   p->defect_passes = build_passes(p, true);
-  for (auto& pc : p->iter_passes)
-    if (2 * (int64_t)p->batch * pc.tiles > p->partials_len) return fail(MMX_ERR_ARG, "internal: partials too small");
+  p->plane_passes = build_plane_passes(p);
+  for (const auto* list : {&p->iter_passes, &p->plane_passes})
+    for (auto& pc : *list)
+      if (2 * (int64_t)p->batch * pc.tiles > p->partials_len) return fail(MMX_ERR_ARG, "internal: partials too small");
   return MMX_OK;
 }
 
 extern "C" unsigned mmx_plan_get_variant(const mmx_plan* p) {
   if (!p) return 0u;
   return (p->force_generic ? MMX_VARIANT_GENERIC : 0u) | (p->no_reg ? MMX_VARIANT_SHARED_STAGED : 0u) |
-         (p->pipe ? MMX_VARIANT_PERSISTENT : 0u);
+         (p->pipe ? MMX_VARIANT_PERSISTENT : 0u) | (p->plane ? MMX_VARIANT_PLANE : 0u);
 }
 
 extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,
