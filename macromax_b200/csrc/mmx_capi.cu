@@ -321,7 +321,7 @@ int launch_pipe(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   if constexpr (N == 192 || N == 384 || (C == 3 && N > 128)) {
     return fail(MMX_ERR_ARG, "internal: no persistent kernel for this length");
   } else {
-    constexpr int PCK = RegCDefault<C, N>::PC_EPI;
+    constexpr int PCK = RegCDefault<C, N>::PC_PIPE;
     auto kern = k_pipe_pass<C, OPS, N, PCK>;
     const size_t smem = PipeLayout<C, OPS, N, PCK>::bytes();
     static int configured_mask = 0;
@@ -479,19 +479,18 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
         }
         int pcp = 1;
         switch (n * 4 + p->ncomp) {
-          case 64 * 4 + 1: pcp = RegCDefault<1, 64>::PC_EPI; break;
-          case 128 * 4 + 1: pcp = RegCDefault<1, 128>::PC_EPI; break;
-          case 256 * 4 + 1: pcp = RegCDefault<1, 256>::PC_EPI; break;
-          case 512 * 4 + 1: pcp = RegCDefault<1, 512>::PC_EPI; break;
-          case 64 * 4 + 3: pcp = RegCDefault<3, 64>::PC_EPI; break;
-          case 128 * 4 + 3: pcp = RegCDefault<3, 128>::PC_EPI; break;
+          case 64 * 4 + 1: pcp = RegCDefault<1, 64>::PC_PIPE; break;
+          case 128 * 4 + 1: pcp = RegCDefault<1, 128>::PC_PIPE; break;
+          case 256 * 4 + 1: pcp = RegCDefault<1, 256>::PC_PIPE; break;
+          case 512 * 4 + 1: pcp = RegCDefault<1, 512>::PC_PIPE; break;
+          case 64 * 4 + 3: pcp = RegCDefault<3, 64>::PC_PIPE; break;
+          case 128 * 4 + 3: pcp = RegCDefault<3, 128>::PC_PIPE; break;
         }
         if (outer % pcp == 0 && p->pipe) pc.pipe = 1;
         if (outer % pcr == 0) {
           pc.regc = 1;
           pc.rc_tiles = outer / pcr;
           pc.rc_smem = ((size_t)p->ncomp * pcr * (n + n / 16) + n) * sizeof(float2);
-          if (epi) pc.rc_smem += (size_t)(p->ncomp + 1) * pcr * n * sizeof(float2);  // staged E and chi
         }
       }
       if (strided_op && inner % kRegP == 0 && reg_length(n, p->ncomp) && !p->no_reg) {

@@ -45,10 +45,6 @@ __device__ __forceinline__ int ridx(int n, int m) { return n * PITCH + col(m); }
 
 inline size_t smem_bytes() { return ((size_t)H * PITCH + N) * sizeof(float2); }
 
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
 // Swap the off-diagonal quarter with the peer CTA: our S[*][col(64 p + j)] <- peer's S[*][col(64 r + j)].
 __device__ __forceinline__ void swap_quarter(float2* sm, cooperative_groups::cluster_group& cluster, int r) {
   const int p = r ^ 1;

@@ -192,7 +192,10 @@ template <int C, int N> struct RegCDefault {
   static constexpr int TPP = RegPlan<N>::TPP;
   static constexpr int P0 = 384 / (C * TPP);
   static constexpr int PC = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : P0 >= 4 ? 4 : P0 >= 2 ? 2 : 1;
-  static constexpr int PC_EPI = PC >= 2 ? PC / 2 : 1;  // the epilogue also stages E and chi in shared memory
+  // epilogue: at most 256 threads per CTA (it runs with more CTAs per SM)
+  static constexpr int PE0 = 256 / (C * TPP);
+  static constexpr int PC_EPI = PE0 >= 32 ? 32 : PE0 >= 16 ? 16 : PE0 >= 8 ? 8 : PE0 >= 4 ? 4 : PE0 >= 2 ? 2 : 1;
+  static constexpr int PC_PIPE = PC >= 2 ? PC / 2 : 1;  // persistent variant: also stages its inputs in smem
 };
 
 template <int C, int N, int PC_> struct RegC {
@@ -238,6 +241,11 @@ __device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, unsi
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
                "l"(gsrc), "r"(bytes), "r"(b)
                : "memory");
+}
+
+// bulk prefetch of a contiguous global range into L2 (16-byte aligned address, size a multiple of 16)
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 // in-place shared-memory stage for the contiguous layout
@@ -321,8 +329,16 @@ template <int... Rs> struct RegPlanArgs<RegPlanList<Rs...>> {
   };
 };
 
+// Resident CTAs per SM the register budget is sized for: the prologue keeps two (it holds three input streams per
+// butterfly); the epilogue targets 64 registers per thread, i.e. 1024 threads per SM.
+template <int C, int OPS, int N, int PC_> struct RegCMinBlocks {
+  static constexpr int T = RegC<C, N, PC_>::THREADS;
+  static constexpr int value = (OPS & OP_EPI) ? (1024 / T >= 2 ? 1024 / T : 2) : 2;
+};
+
 template <int C, int OPS, int N, int PC_>
-__global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, 2) k_regc_pass(IterArgs<float> a) {
+__global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OPS, N, PC_>::value))
+    k_regc_pass(IterArgs<float> a) {
   using G = RegC<C, N, PC_>;
   using PA = RegPlanArgs<typename RegPlan<N>::type>;
   constexpr int TPP = G::TPP, PC = G::PC, THREADS = G::THREADS;
@@ -390,19 +406,15 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, 2) k_regc_pass(IterA
       for (int q = 0; q < RL; ++q) a.T[fbase + c * N3 + rowbase + i + q * LL] = v[m][q];
     }
   } else {
-    // INV | EPI.  E and chi of the tile's rows are contiguous chunks (PC rows x N samples per component): fetch
-    // them with bulk copies into shared memory now, so they arrive while the inverse transform of T runs.
-    float2* smE = smtw + N;              // [C][PC][N]
-    float2* smX = smE + C * PC * N;      // [PC][N]
-    __shared__ __align__(8) uint64_t bar;
-    const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
-    const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+    // INV | EPI.  E and chi of the tile's rows are contiguous chunks (PC rows x N samples per component): a bulk
+    // L2 prefetch issued now brings them on chip while the inverse transform of T runs; the last stage then reads
+    // them with plain loads.
     if (tid == 0) {
-      mbar_init(&bar, 1);
-      mbar_expect_tx(&bar, chunk * (C + 1));
+      const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+      const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
 #pragma unroll
-      for (int cc2 = 0; cc2 < C; ++cc2) bulk_load(smE + cc2 * PC * N, Ecur + fbase + cc2 * N3 + row0, chunk, &bar);
-      bulk_load(smX, a.chi + row0, chunk, &bar);
+      for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
+      prefetch_l2(a.chi + row0, chunk);
     }
     // first stage from T (global) into shared memory
     constexpr int RAD = PA::R_first;
@@ -429,34 +441,30 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, 2) k_regc_pass(IterA
     constexpr int NBL = TL / TPP;
     constexpr int LL = N / RL;
     double dd2 = 0.0, en2 = 0.0;
-    const bool staged = mbar_wait(&bar, 0);  // bounded: on a timeout, fall back to global loads
-    const float2* eS = staged ? smE + (c * PC + row) * N : Ecur + fbase + c * N3 + rowbase;
-    const float2* xS = staged ? smX + row * N : a.chi + rowbase;
-    float2 v[NBL][RL];
-#pragma unroll
+    const float2* __restrict__ eS = Ecur + fbase + c * N3 + rowbase;
+    const float2* __restrict__ xS = a.chi + rowbase;
+    float2* __restrict__ eO = Eoth + fbase + c * N3 + rowbase;
+    // one butterfly at a time: its RL outputs, then RL epilogue words, keep the live registers low
+#pragma unroll 1
     for (int m = 0; m < NBL; ++m) {
       const int i = ii + m * TPP;
+      float2 v[RL];
 #pragma unroll
-      for (int q = 0; q < RL; ++q) v[m][q] = sm[G::idx(c, row, i + q * TL)];
+      for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
 #pragma unroll
-      for (int q = 1; q < RL; ++q) v[m][q] = v[m][q] * conjc(smtw[q * i]);
-      bfly<float, RL, +1>(v[m], smtw, N);
+      for (int q = 1; q < RL; ++q) v[q] = v[q] * conjc(smtw[q * i]);
+      bfly<float, RL, +1>(v, smtw, N);
 #pragma unroll
       for (int q = 0; q < RL; ++q) {
         const int s_ = i + q * LL;
         const float2 e = eS[s_];
         const float2 x = cc.a * xS[s_] + cc.b;
-        const float2 d = x * (v[m][q] - e);
+        const float2 d = x * (v[q] - e);
         const float2 en = e + d;
-        Eoth[fbase + c * N3 + rowbase + s_] = en;
+        eO[s_] = en;
         dd2 += norm2d(d);
         en2 += norm2d(en);
       }
-    }
-    if (!staged && tid == 0) {
-      // the bulk copy did not complete in time: flag it and drain it (bounded) before the block exits
-      atomicOr(&const_cast<mmx_rhs_state*>(st)->status, MMX_STATUS_TIMEOUT);
-      mbar_wait(&bar, 0);
     }
     finish_pass_norms(a, b, dd2, en2);
   }
