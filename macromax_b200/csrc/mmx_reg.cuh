@@ -190,12 +190,14 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
 // ---------------------------------------------------------------------------------------------------------------
 template <int C, int N> struct RegCDefault {
   static constexpr int TPP = RegPlan<N>::TPP;
-  static constexpr int P0 = 384 / (C * TPP);
+  // prologue and epilogue tiles: at most 256 threads per CTA, several CTAs per SM
+  static constexpr int P0 = 256 / (C * TPP);
   static constexpr int PC = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : P0 >= 4 ? 4 : P0 >= 2 ? 2 : 1;
-  // epilogue: at most 256 threads per CTA (it runs with more CTAs per SM)
-  static constexpr int PE0 = 256 / (C * TPP);
-  static constexpr int PC_EPI = PE0 >= 32 ? 32 : PE0 >= 16 ? 16 : PE0 >= 8 ? 8 : PE0 >= 4 ? 4 : PE0 >= 2 ? 2 : 1;
-  static constexpr int PC_PIPE = PC >= 2 ? PC / 2 : 1;  // persistent variant: also stages its inputs in smem
+  static constexpr int PC_EPI = PC;
+  // persistent variant (one CTA per SM, stages its inputs in shared memory): 384-thread budget, half the rows
+  static constexpr int PP0 = 384 / (C * TPP);
+  static constexpr int PC_PIPE0 = PP0 >= 32 ? 32 : PP0 >= 16 ? 16 : PP0 >= 8 ? 8 : PP0 >= 4 ? 4 : PP0 >= 2 ? 2 : 1;
+  static constexpr int PC_PIPE = PC_PIPE0 >= 2 ? PC_PIPE0 / 2 : 1;
 };
 
 template <int C, int N, int PC_> struct RegC {
@@ -329,11 +331,10 @@ template <int... Rs> struct RegPlanArgs<RegPlanList<Rs...>> {
   };
 };
 
-// Resident CTAs per SM the register budget is sized for: the prologue keeps two (it holds three input streams per
-// butterfly); the epilogue targets 64 registers per thread, i.e. 1024 threads per SM.
+// Resident CTAs per SM the register budget is sized for: 64 registers per thread, i.e. 1024 threads per SM.
 template <int C, int OPS, int N, int PC_> struct RegCMinBlocks {
   static constexpr int T = RegC<C, N, PC_>::THREADS;
-  static constexpr int value = (OPS & OP_EPI) ? (1024 / T >= 2 ? 1024 / T : 2) : 2;
+  static constexpr int value = 1024 / T >= 2 ? 1024 / T : 2;
 };
 
 template <int C, int OPS, int N, int PC_>
@@ -364,46 +365,57 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
   __syncthreads();
 
   if constexpr (OPS == (OP_PRO | OP_FWD)) {
-    // first stage: x = chi E + s' from global, radix R_first, L = 1, outputs to shared memory
+    // E, s' and chi of the tile's rows are contiguous chunks: prefetch them into L2 in bulk
+    if (tid == 0) {
+      const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+      const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
+#pragma unroll
+      for (int cc2 = 0; cc2 < C; ++cc2) {
+        prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
+        prefetch_l2(a.src + fbase + cc2 * N3 + row0, chunk);
+      }
+      prefetch_l2(a.chi + row0, chunk);
+    }
+    // first stage: x = chi E + s' from global, radix R_first, L = 1, outputs to shared memory, one butterfly at a
+    // time (the source is global memory, so each butterfly can be stored as soon as it is done)
     constexpr int RAD = PA::R_first;
     constexpr int T = N / RAD;
     constexpr int NBT = T / TPP;
-    float2 u[NBT][RAD];
-#pragma unroll
+    const float2* __restrict__ eS = Ecur + fbase + c * N3 + rowbase;
+    const float2* __restrict__ sS = a.src + fbase + c * N3 + rowbase;
+    const float2* __restrict__ xS = a.chi + rowbase;
+#pragma unroll 1
     for (int m = 0; m < NBT; ++m) {
       const int i = ii + m * TPP;
+      float2 u[RAD];
 #pragma unroll
       for (int q = 0; q < RAD; ++q) {
-        const int64_t vox = rowbase + i + q * T;
-        const float2 x = cc.a * a.chi[vox] + cc.b;
-        u[m][q] = x * Ecur[fbase + c * N3 + vox] + cc.s * a.src[fbase + c * N3 + vox];
+        const int s_ = i + q * T;
+        u[q] = (cc.a * xS[s_] + cc.b) * eS[s_] + cc.s * sS[s_];
       }
-      bfly<float, RAD, -1>(u[m], smtw, N);
-    }
+      bfly<float, RAD, -1>(u, smtw, N);
 #pragma unroll
-    for (int m = 0; m < NBT; ++m) {
-      const int i = ii + m * TPP;
-#pragma unroll
-      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[m][q];
+      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[q];
     }
     __syncthreads();
     PA::template mid<-1, N, C, PC>(sm, smtw);
-    // last stage: shared -> registers -> T (global)
+    // last stage: shared -> registers -> T (global), one butterfly at a time
     constexpr int RL = PA::R_last;
     constexpr int TL = N / RL;
     constexpr int NBL = TL / TPP;
     constexpr int LL = N / RL;
-    float2 v[NBL][RL];
-#pragma unroll
+    float2* __restrict__ tO = a.T + fbase + c * N3 + rowbase;
+#pragma unroll 1
     for (int m = 0; m < NBL; ++m) {
       const int i = ii + m * TPP;
+      float2 v[RL];
 #pragma unroll
-      for (int q = 0; q < RL; ++q) v[m][q] = sm[G::idx(c, row, i + q * TL)];
+      for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
 #pragma unroll
-      for (int q = 1; q < RL; ++q) v[m][q] = v[m][q] * smtw[q * i];
-      bfly<float, RL, -1>(v[m], smtw, N);
+      for (int q = 1; q < RL; ++q) v[q] = v[q] * smtw[q * i];
+      bfly<float, RL, -1>(v, smtw, N);
 #pragma unroll
-      for (int q = 0; q < RL; ++q) a.T[fbase + c * N3 + rowbase + i + q * LL] = v[m][q];
+      for (int q = 0; q < RL; ++q) tO[i + q * LL] = v[q];
     }
   } else {
     // INV | EPI.  E and chi of the tile's rows are contiguous chunks (PC rows x N samples per component): a bulk
