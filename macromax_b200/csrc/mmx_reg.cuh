@@ -91,6 +91,96 @@ __device__ __forceinline__ void rfft(float2* sm, const float2* tw, const float2*
   rstages<DIR, N, C, FIRST_G, LAST_G, 1, Rs...>(sm, tw, gsrc, gdst, js, cs);
 }
 
+// Radix-plan list algebra: concatenation, reversal, all-but-last and last.
+template <class A, class B> struct PlanConcat;
+template <int... A, int... B> struct PlanConcat<RegPlanList<A...>, RegPlanList<B...>> {
+  using type = RegPlanList<A..., B...>;
+};
+template <class L> struct PlanReverse;
+template <> struct PlanReverse<RegPlanList<>> { using type = RegPlanList<>; };
+template <int R0, int... Rs> struct PlanReverse<RegPlanList<R0, Rs...>> {
+  using type = typename PlanConcat<typename PlanReverse<RegPlanList<Rs...>>::type, RegPlanList<R0>>::type;
+};
+template <class L> struct PlanInit;
+template <int R0> struct PlanInit<RegPlanList<R0>> { using type = RegPlanList<>; };
+template <int R0, int R1, int... Rs> struct PlanInit<RegPlanList<R0, R1, Rs...>> {
+  using type = typename PlanConcat<RegPlanList<R0>, typename PlanInit<RegPlanList<R1, Rs...>>::type>::type;
+};
+template <class L> struct PlanLast;
+template <int R0> struct PlanLast<RegPlanList<R0>> { static constexpr int value = R0; };
+template <int R0, int R1, int... Rs> struct PlanLast<RegPlanList<R0, R1, Rs...>> {
+  static constexpr int value = PlanLast<RegPlanList<R1, Rs...>>::value;
+};
+
+// The stages of `List` in order, the first one at span L (FIRST_G: it reads global memory; LAST_G: the last one
+// writes global memory).
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, class List> struct RChain;
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L>
+struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<>> {
+  static __device__ __forceinline__ void run(float2*, const float2*, const float2*, float2*, int64_t, int64_t) {}
+};
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, int R0, int... Rs>
+struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<R0, Rs...>> {
+  static __device__ __forceinline__ void run(float2* sm, const float2* tw, const float2* gsrc, float2* gdst,
+                                             int64_t js, int64_t cs) {
+    constexpr bool last = sizeof...(Rs) == 0;
+    rstage<DIR, N, C, R0, L, FIRST_G, LAST_G && last>(sm, tw, gsrc, gdst, js, cs);
+    RChain<DIR, N, C, false, LAST_G, L * R0, RegPlanList<Rs...>>::run(sm, tw, gsrc, gdst, js, cs);
+  }
+};
+
+// Last forward stage (radix R, span N / R), the scalar Green multiply and the first inverse stage (radix R, span 1)
+// of a 16-pencil tile, in registers.  The last forward stage of butterfly i writes the positions i + q N / R, which
+// are exactly the inputs of butterfly i of the first inverse stage when the inverse runs the radix plan in reverse
+// order; so the spectrum never goes back to shared memory between the two transforms.
+//   g(k) = -i a_i / (|k|^2 - a) / N  (solver.py:566-568, with the 1/N of the inverse transform)
+template <int N, int R>
+__device__ __forceinline__ void green_fused_scalar(float2* sm, const float2* tw, const float* sk0, const float* sk1,
+                                                   const float* sk2, float ar, float ai, float ai2s, float ais) {
+  constexpr int P = kRegP, TPP = RegPlan<N>::TPP, T = N / R, NB = T / TPP;
+  static_assert(NB >= 1 && T % TPP == 0, "stage does not split evenly over the threads");
+  // The stage reads positions i + q T and writes i R + q of the same pencil, so all of a pencil's reads precede its
+  // writes.  At 512 samples it runs in NB rounds over P / NB pencils each, one butterfly per thread and round, which
+  // keeps the kernel within its register budget; otherwise each thread holds its NB butterflies at once.
+  constexpr int ROUNDS = (N == 512) ? NB : 1;
+  constexpr int PR = P / ROUNDS;    // pencils per round
+  constexpr int NBR = NB / ROUNDS;  // butterflies per thread and round
+  const int tid = threadIdx.x;
+  const float ai2 = ai * ai;
+#pragma unroll 1
+  for (int rd = 0; rd < ROUNDS; ++rd) {
+    const int pl = rd * PR + tid % PR;
+    const int ii = (tid / PR) % (TPP * ROUNDS);
+    const float kt2 = sk1[pl] * sk1[pl] + sk2[pl] * sk2[pl];
+    float2 u[NBR][R];
+#pragma unroll
+    for (int m = 0; m < NBR; ++m) {
+      const int i = ii + m * TPP * ROUNDS;
+#pragma unroll
+      for (int q = 0; q < R; ++q) u[m][q] = sm[(i + q * T) * P + pl];
+#pragma unroll
+      for (int q = 1; q < R; ++q) u[m][q] = u[m][q] * tw[q * i];
+      bfly<float, R, -1>(u[m], tw, N);
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const float k0 = sk0[i + q * T];
+        const float dr = fmaf(k0, k0, kt2) - ar;
+        const float inv = __fdividef(1.f, fmaf(dr, dr, ai2));
+        u[m][q] = u[m][q] * make_float2(ai2s * inv, ais * dr * inv);
+      }
+      bfly<float, R, +1>(u[m], tw, N);
+    }
+    __syncthreads();  // every butterfly of these pencils has read its inputs
+#pragma unroll
+    for (int m = 0; m < NBR; ++m) {
+      const int i = ii + m * TPP * ROUNDS;
+#pragma unroll
+      for (int q = 0; q < R; ++q) sm[(i * R + q) * P + pl] = u[m][q];
+    }
+    __syncthreads();
+  }
+}
+
 // OPS: OP_FWD (forward pass), OP_INV (inverse pass) or OP_FWD | OP_G | OP_INV (axis-0 pass with the Green multiply)
 template <int C, int OPS, int N>
 __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArgs<float> a) {
@@ -117,10 +207,37 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
   } else if constexpr (OPS == OP_INV) {
     rfft<+1, N, C, true, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
   } else {
+    __shared__ float sk1[P], sk2[P], sk0[N];
+    const ChiCoef<float> cc = chi_coef<float>(st);
+    if constexpr (C == 1) {
+      // scalar field: k tables first, then the forward stages but the last, the fused last-forward / Green /
+      // first-inverse stage, and the remaining inverse stages in reverse radix order
+      if (tid < P) {
+        const int64_t p = in0 + tid;
+        float k1 = 0.f, k2 = 0.f;
+        if (a.ndim == 3) {
+          const int i1 = (int)(p / a.dims[2]);
+          const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
+          k1 = a.kv[1][i1];
+          k2 = a.kv[2][i2];
+        } else if (a.ndim == 2) {
+          k1 = a.kv[1][p];
+        }
+        sk1[tid] = k1;
+        sk2[tid] = k2;
+      }
+      for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
+      // (the forward chain's first stage reads global memory only; its closing barrier publishes the tables)
+      using Init = typename PlanInit<Plan>::type;
+      constexpr int RL = PlanLast<Plan>::value;
+      RChain<-1, N, 1, true, false, 1, Init>::run(sm, smtw, tile, tile, inner, a.N);
+      const float ar = cc.alpha_re, ai = cc.alpha_im;
+      green_fused_scalar<N, RL>(sm, smtw, sk0, sk1, sk2, ar, ai, ai * ai * a.inv_total, -ai * a.inv_total);
+      RChain<+1, N, 1, false, true, RL, typename PlanReverse<Init>::type>::run(sm, smtw, tile, tile, inner, a.N);
+      return;
+    }
     // forward transform into shared memory, Green multiply, inverse transform back to global memory
     rfft<-1, N, C, true, false>(sm, smtw, tile, tile, inner, a.N, Plan{});
-    const ChiCoef<float> cc = chi_coef<float>(st);
-    __shared__ float sk1[P], sk2[P], sk0[N];
     if (tid < P) {
       const int64_t p = in0 + tid;
       float k1 = 0.f, k2 = 0.f;
@@ -146,7 +263,7 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
       const float k0 = sk0[j], k1 = sk1[pl], k2 = sk2[pl];
       const float kk2 = k0 * k0 + k1 * k1 + k2 * k2;
       const float dr = kk2 - ar;
-      const float inv = 1.f / (dr * dr + ai * ai);
+      const float inv = __fdividef(1.f, fmaf(dr, dr, ai * ai));
       const float2 g = make_float2(ai2s * inv, ais * dr * inv);  // -i a_i / (|k|^2 - a) / N
       if constexpr (C == 1) {
         sm[j * P + pl] = sm[j * P + pl] * g;
@@ -163,7 +280,7 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
 #pragma unroll
           for (int c = 0; c < 3; ++c)
             if (c < a.ndim) proj += kv[c] * F[c];
-          proj = proj * (1.f / kk2);
+          proj = proj * __fdividef(1.f, kk2);
 #pragma unroll
           for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? kv[c] * proj : make_float2(0.f, 0.f);
         }
