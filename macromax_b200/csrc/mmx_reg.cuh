@@ -181,6 +181,74 @@ __device__ __forceinline__ void green_fused_scalar(float2* sm, const float2* tw,
   }
 }
 
+// The same fused stage for a 3-component field: one thread takes all three components of a (pencil, butterfly) item,
+// so that the dyadic Green multiply (backend/__init__.py:606-649 longitudinal projection, solver.py:571-577) sees
+// the whole vector at each k:  F' = g (F - P_L F) + (i alpha_i / alpha) P_L F / N,  P_L = k k^T / |k|^2, with the
+// DC rule of the reference (P_L F = F on the grid's axes at k = 0) and no longitudinal part along absent axes.
+// The P x (N / R) items are spread over the first threads of the block; the others only join the barriers.
+template <int N, int R>
+__device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw, const float* sk0, const float* sk1,
+                                                   const float* sk2, bool dc_tile, int ndim, float ar, float ai,
+                                                   float ai2s, float ais, float2 hs) {
+  constexpr int P = kRegP, T = N / R, ITEMS = P * T;
+  constexpr int THREADS = RegThreads<3, N>::value;
+  static_assert(ITEMS <= THREADS, "one item per thread");
+  const int tid = threadIdx.x;
+  const int pl = tid % P;
+  const int i = tid / P;
+  const bool active = tid < ITEMS;
+  float2 u[3][R];
+  if (active) {
+    const float k1 = sk1[pl], k2 = sk2[pl];
+    const float kt2 = k1 * k1 + k2 * k2;
+    const float ai2 = ai * ai;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) u[c][q] = sm[(c * N + i + q * T) * P + pl];
+#pragma unroll
+      for (int q = 1; q < R; ++q) u[c][q] = u[c][q] * tw[q * i];
+      bfly<float, R, -1>(u[c], tw, N);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int j = i + q * T;
+      const float k0 = sk0[j];
+      const float kk2 = fmaf(k0, k0, kt2);
+      const float dr = kk2 - ar;
+      const float inv = __fdividef(1.f, fmaf(dr, dr, ai2));
+      const float2 g = make_float2(ai2s * inv, ais * dr * inv);
+      const float kv[3] = {k0, k1, k2};
+      float2 PL[3];
+      if (dc_tile && j == 0 && pl == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) PL[c] = c < ndim ? u[c][q] : make_float2(0.f, 0.f);
+      } else {
+        float2 proj = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          if (c < ndim) proj += kv[c] * u[c][q];
+        proj = proj * __fdividef(1.f, kk2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) PL[c] = c < ndim ? kv[c] * proj : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u[c][q] = g * (u[c][q] - PL[c]) + hs * PL[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) bfly<float, R, +1>(u[c], tw, N);
+  }
+  __syncthreads();  // every item has read its inputs
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) sm[(c * N + i * R + q) * P + pl] = u[c][q];
+    }
+  }
+  __syncthreads();
+}
+
 // OPS: OP_FWD (forward pass), OP_INV (inverse pass) or OP_FWD | OP_G | OP_INV (axis-0 pass with the Green multiply)
 template <int C, int OPS, int N>
 __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArgs<float> a) {
@@ -234,6 +302,32 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
       const float ar = cc.alpha_re, ai = cc.alpha_im;
       green_fused_scalar<N, RL>(sm, smtw, sk0, sk1, sk2, ar, ai, ai * ai * a.inv_total, -ai * a.inv_total);
       RChain<+1, N, 1, false, true, RL, typename PlanReverse<Init>::type>::run(sm, smtw, tile, tile, inner, a.N);
+      return;
+    } else if constexpr (C == 3 && N == 128) {
+      // vector field: the same fused schedule with the dyadic Green multiply (all three components per item)
+      if (tid < P) {
+        const int64_t p = in0 + tid;
+        float k1 = 0.f, k2 = 0.f;
+        if (a.ndim == 3) {
+          const int i1 = (int)(p / a.dims[2]);
+          const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
+          k1 = a.kv[1][i1];
+          k2 = a.kv[2][i2];
+        } else if (a.ndim == 2) {
+          k1 = a.kv[1][p];
+        }
+        sk1[tid] = k1;
+        sk2[tid] = k2;
+      }
+      for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
+      using Init = typename PlanInit<Plan>::type;
+      constexpr int RL = PlanLast<Plan>::value;
+      RChain<-1, N, 3, true, false, 1, Init>::run(sm, smtw, tile, tile, inner, a.N);
+      const float ar = cc.alpha_re, ai = cc.alpha_im;
+      const float2 hs = divc(make_float2(0.f, ai), make_float2(ar, ai)) * a.inv_total;
+      green_fused_vector<N, RL>(sm, smtw, sk0, sk1, sk2, in0 == 0, a.ndim, ar, ai, ai * ai * a.inv_total,
+                                -ai * a.inv_total, hs);
+      RChain<+1, N, 3, false, true, RL, typename PlanReverse<Init>::type>::run(sm, smtw, tile, tile, inner, a.N);
       return;
     }
     // forward transform into shared memory, Green multiply, inverse transform back to global memory
