@@ -39,6 +39,32 @@ int cuda_fail(cudaError_t e, const char* what) {
 
 constexpr size_t kSmemCap = 220 * 1024;
 
+// Pass kernels are launched with programmatic stream serialization (the next pass may be scheduled while the
+// previous one drains; the kernels wait for their predecessor's memory, see pdl_wait).  MMX_NO_PDL=1 turns it off.
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = getenv("MMX_NO_PDL");
+    return !(v && v[0] == '1');
+  }();
+  return on;
+}
+
+template <class... KArgs, class... Args>
+cudaError_t launch_pass(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                        Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 struct PassCfg {
   int axis;
   int ops;
@@ -252,7 +278,7 @@ int launch_fast(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
     cfg.numAttrs = 1;
     MMX_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
   } else {
-    kern<<<grid, FastThreads<C, N, kFastP>::value, pc.smem, s>>>(a);
+    MMX_CUDA(launch_pass(kern, grid, dim3(FastThreads<C, N, kFastP>::value), pc.smem, s, a));
   }
   MMX_CUDA(cudaGetLastError());
   return MMX_OK;
@@ -276,7 +302,7 @@ int launch_reg(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) 
     a.P = kRegP;
     a.sP = kRegP;
     dim3 grid((unsigned)pc.tiles, (unsigned)batch);
-    kern<<<grid, RegThreads<C, N>::value, pc.smem, s>>>(a);
+    MMX_CUDA(launch_pass(kern, grid, dim3(RegThreads<C, N>::value), pc.smem, s, a));
     MMX_CUDA(cudaGetLastError());
     return MMX_OK;
   }
@@ -299,7 +325,7 @@ int launch_regc(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
     a.outer = pc.outer;
     a.inner = pc.inner;
     dim3 grid((unsigned)pc.rc_tiles, (unsigned)batch);
-    kern<<<grid, RegC<C, N, PCK>::THREADS, pc.rc_smem, s>>>(a);
+    MMX_CUDA(launch_pass(kern, grid, dim3(RegC<C, N, PCK>::THREADS), pc.rc_smem, s, a));
     MMX_CUDA(cudaGetLastError());
     return MMX_OK;
   }
@@ -358,7 +384,7 @@ int launch_plane(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s
   a.outer = pc.outer;
   a.inner = pc.inner;
   dim3 grid((unsigned)pc.tiles, (unsigned)batch);  // tiles = 2 n0 C (two CTAs per component plane)
-  kern<<<grid, mmx_plane::THREADS, smem, s>>>(a);
+  MMX_CUDA(launch_pass(kern, grid, dim3(mmx_plane::THREADS), smem, s, a));
   MMX_CUDA(cudaGetLastError());
   return MMX_OK;
 }

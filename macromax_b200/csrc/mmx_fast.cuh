@@ -95,6 +95,8 @@ __global__ void __launch_bounds__(FastThreads<C, N, P>::value, 2) k_fast_pass(It
   float2* smtw = sm + C * N * SP;  // twiddle table copy [N]
   const int b = blockIdx.y;
   const mmx_rhs_state* st = a.st + b;
+  pdl_wait();
+  pdl_trigger();
   if (!st->active) return;
   const ChiCoef<R> cc = chi_coef<R>(st);
   const int tid = threadIdx.x;

@@ -47,6 +47,14 @@ template <class R> struct IterArgs {
   int nrhs;              // number of right-hand sides (persistent passes)
 };
 
+// Programmatic dependent launch.  The pass kernels are launched so that the next pass's CTAs may become resident
+// while this grid drains; each pass calls pdl_wait() before it reads anything an earlier kernel writes (the fields,
+// the work buffer, the right-hand-side state), which returns once those grids have completed and their memory is
+// visible.  pdl_trigger() lets the dependent grid be scheduled as soon as every CTA of this grid has started.
+// Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // |z|^2 accumulated in FP64 (the squares of complex64 words are exact in double)
 __device__ __forceinline__ double norm2d(float2 z) { return (double)z.x * z.x + (double)z.y * z.y; }
 __device__ __forceinline__ double norm2d(double2 z) { return z.x * z.x + z.y * z.y; }

@@ -89,6 +89,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(mmx_plane::THREADS, 
   cg::cluster_group cluster = cg::this_cluster();
   const int b = blockIdx.y;
   const mmx_rhs_state* st = a.st + b;
+  pdl_wait();
+  pdl_trigger();
   if (!st->active) return;  // both CTAs of a cluster share b, so both leave
   const int r = (int)cluster.block_rank();
   const int tid = threadIdx.x;

@@ -259,6 +259,8 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
   float2* smtw = sm + C * N * P;
   const int b = blockIdx.y;
   const mmx_rhs_state* st = a.st + b;
+  pdl_wait();
+  pdl_trigger();
   if (!st->active) return;
   const int tid = threadIdx.x;
   const int64_t inner = a.inner;
@@ -559,6 +561,19 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
   float2* smtw = sm + C * PC * G::PITCH;
   const int b = blockIdx.y;
   const mmx_rhs_state* st = a.st + b;
+  if (threadIdx.x == 0) {
+    // inputs no kernel writes (chi, and s' for the prologue): prefetch them into L2 before waiting for the
+    // previous pass; the fields follow once the state says which buffer is current
+    const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+    const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
+    prefetch_l2(a.chi + row0, chunk);
+    if constexpr ((OPS & OP_PRO) != 0) {
+#pragma unroll
+      for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(a.src + ((int64_t)b * C + cc2) * a.N + row0, chunk);
+    }
+  }
+  pdl_wait();
+  pdl_trigger();
   if (!st->active) return;
   const ChiCoef<float> cc = chi_coef<float>(st);
   const int tid = threadIdx.x;
@@ -581,11 +596,7 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
       const int64_t row0 = (int64_t)blockIdx.x * PC * N;
       const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
 #pragma unroll
-      for (int cc2 = 0; cc2 < C; ++cc2) {
-        prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
-        prefetch_l2(a.src + fbase + cc2 * N3 + row0, chunk);
-      }
-      prefetch_l2(a.chi + row0, chunk);
+      for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
     }
     // first stage: x = chi E + s' from global, radix R_first, L = 1, outputs to shared memory, one butterfly at a
     // time (the source is global memory, so each butterfly can be stored as soon as it is done)
@@ -637,7 +648,6 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
       const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
 #pragma unroll
       for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
-      prefetch_l2(a.chi + row0, chunk);
     }
     // first stage from T (global) into shared memory
     constexpr int RAD = PA::R_first;
