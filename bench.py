@@ -338,10 +338,13 @@ def run_secondary(args):
     torch.cuda.synchronize()
     c = time.perf_counter()
     fi, ai = stats['forward_iterations'], stats['adjoint_iterations']
+    solve_s = stats['forward_solve_s'] + stats['adjoint_solve_s']
     out['adjoint_design3d_128x32'] = {
         'forward_s': b - a, 'backward_s': c - b, 'forward_iterations_max': int(fi.max()),
         'adjoint_iterations_max': int(ai.max()),
-        'voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / (c - a)}
+        'voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / (c - a),
+        'solve_s (forward + adjoint iterations only)': solve_s,
+        'solve_voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / solve_s}
     return out
 
 

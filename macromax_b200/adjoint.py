@@ -18,6 +18,7 @@ iteration (examples/scattering_neural_network.py:206-300).
 from __future__ import annotations
 
 import ctypes
+import time
 
 import numpy as np
 import torch
@@ -31,6 +32,12 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _now() -> float:
+    """Host time after the device has finished the work queued so far (solve-phase timing in ``stats``)."""
+    torch.cuda.synchronize()
+    return time.perf_counter()
+
+
 def _stream():
     s = torch.cuda.current_stream().cuda_stream
     return ctypes.c_void_p(s) if s else None
@@ -40,12 +47,15 @@ class _SolveFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, epsilon, sources, problem):
         grid, k0 = problem['grid'], problem['wavenumber']
+        # the permittivity goes to the host for the FP64 preconditioner set-up (as in the reference); the sources
+        # stay on the device
         eps_np = epsilon.detach().cpu().numpy()
-        src_np = sources.detach().cpu().numpy()
-        bs = BatchSolution(grid, src_np, eps_np, bound=problem.get('bound'), wavenumber=k0,
+        bs = BatchSolution(grid, sources.detach(), eps_np, bound=problem.get('bound'), wavenumber=k0,
                            dtype=problem.get('dtype', np.complex64), device=sources.device)
+        t0 = _now()
         bs.solve(problem.get('rtol', 1e-6), problem.get('maxiter', 100000))
         problem.setdefault('stats', {})['forward_iterations'] = bs.iterations
+        problem['stats']['forward_solve_s'] = _now() - t0
         E = bs.E_device.clone()  # [B, C, N], k0^2-scaled
         ctx.bs = bs
         ctx.problem = problem
@@ -68,8 +78,10 @@ class _SolveFn(torch.autograd.Function):
         bs.engine.reset_alpha()
         bs.engine.reset_update_norm()
         bs.set_fields(0.0)
+        t0 = _now()
         bs.solve(problem.get('rtol', 1e-6), problem.get('maxiter', 100000))
         problem['stats']['adjoint_iterations'] = bs.iterations
+        problem['stats']['adjoint_solve_s'] = _now() - t0
         nu = bs.E_device  # [B, C, N]
         grad_eps = grad_src = None
         if ctx.needs_input_grad[0]:

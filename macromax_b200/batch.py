@@ -17,6 +17,7 @@ from math import inf
 
 import numpy as np
 import scipy.constants as const
+import torch
 
 from . import _native as nat
 from . import preconditioner as pc
@@ -61,13 +62,14 @@ class BatchSolution:
         self.grid = grid
         self.wavenumber = 2 * np.pi / vacuum_wavelength if vacuum_wavelength is not None else float(wavenumber)
         self.dtype = np.dtype(dtype)
-        src = np.asarray(sources)
+        # a torch tensor (e.g. already on the device) is used as it is; anything else goes through numpy
+        src = sources if isinstance(sources, torch.Tensor) else np.asarray(sources)
         if src.ndim == grid.ndim + 1:
-            src = src[np.newaxis]
+            src = src[None]
         if src.ndim != grid.ndim + 2:
             raise ValueError('sources must be [B, 1|3, *grid]')
-        self.batch = src.shape[0]
-        self.ncomp = src.shape[1]
+        self.batch = int(src.shape[0])
+        self.ncomp = int(src.shape[1])
         if self.ncomp not in (1, 3):
             raise ValueError('sources need 1 or 3 components')
         if preconditioner is None:
@@ -86,11 +88,22 @@ class BatchSolution:
 
     def set_sources(self, src):
         """s'0 = i s / (alpha0_i beta) (solver.py:702-720); resets every previous_update_norm."""
-        src = np.asarray(src)
-        self.engine.set_sources(src * (1.0j / self.pre.alpha.imag / self.pre.beta))
+        scale = 1.0j / self.pre.alpha.imag / self.pre.beta
+        if isinstance(src, torch.Tensor):
+            self.engine.set_sources(src.to(self.engine.device, self.engine.torch_dtype) * scale)
+        else:
+            self.engine.set_sources(np.asarray(src) * scale)
         self.engine.reset_update_norm()
 
     def set_fields(self, E=0.0):
+        if np.isscalar(E):  # a constant field is filled on the device (no host array of the batch's size)
+            E = torch.full((1, self.ncomp, self.engine.N), complex(E) * self.wavenumber ** 2,
+                           dtype=self.engine.torch_dtype, device=self.engine.device)
+            self.engine.set_fields(E)
+            return
+        if isinstance(E, torch.Tensor):
+            self.engine.set_fields(E.reshape(-1, self.ncomp, self.engine.N) * self.wavenumber ** 2)
+            return
         E = np.broadcast_to(np.asarray(E), (self.batch, self.ncomp, *self.grid.shape))
         self.engine.set_fields(E * self.wavenumber ** 2)
 
@@ -170,7 +183,6 @@ class UnevenBatch:
 
     def iterate(self, niter: int):
         import ctypes
-        import torch
         s = torch.cuda.current_stream().cuda_stream
         nat.call('mmx_iterate_multi', *self._args, int(niter), ctypes.c_void_p(s) if s else None)
 

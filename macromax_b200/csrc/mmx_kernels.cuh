@@ -316,10 +316,36 @@ __global__ void __launch_bounds__(512, 2) k_iter_pass(IterArgs<R> a) {
 // 1112-1121) for one right-hand side, from the epilogue pass partials (deterministic fixed-order reduction).
 // Executed by one whole block.
 __device__ void decide_rhs(mmx_rhs_state* S, const double* __restrict__ pp, int ntiles) {
+  // The block is the only one still running when it gets here, so the reduction is on the critical path: every
+  // thread issues its loads U at a time into U independent accumulators (a fixed order for a given ntiles and
+  // block size, hence deterministic) instead of one dependent load-add chain.
+  constexpr int U = 8;
+  const double2* __restrict__ p2 = reinterpret_cast<const double2*>(pp);
+  const int nt = blockDim.x;
+  double sd[U], se[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) sd[u] = se[u] = 0.0;
+  int i = threadIdx.x;
+  for (; i + (U - 1) * nt < ntiles; i += U * nt) {
+    double2 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = p2[i + u * nt];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      sd[u] += v[u].x;
+      se[u] += v[u].y;
+    }
+  }
+  for (int u = 0; i < ntiles; i += nt, ++u) {
+    const double2 v = p2[i];
+    sd[u & (U - 1)] += v.x;
+    se[u & (U - 1)] += v.y;
+  }
   double dd2 = 0.0, en2 = 0.0;
-  for (int i = threadIdx.x; i < ntiles; i += blockDim.x) {
-    dd2 += pp[2 * i];
-    en2 += pp[2 * i + 1];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    dd2 += sd[u];
+    en2 += se[u];
   }
   double out2[2];
   block_reduce_2<double>(dd2, en2, out2);
