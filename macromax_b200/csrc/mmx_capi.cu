@@ -13,6 +13,7 @@
 #include "mmx_fast.cuh"
 #include "mmx_reg.cuh"
 #include "mmx_plane.cuh"
+#include "mmx_epro.cuh"
 
 #define MMX_ABI_VERSION 1
 
@@ -77,6 +78,8 @@ struct PassCfg {
   int regc = 0;  // 1: register-staged contiguous prologue/epilogue pass (k_regc_pass) for an isotropic chi
   int pipe = 0;  // 1: persistent double-buffered variant of the same pass (k_pipe_pass)
   int plane = 0; // 1: plane pass over the two inner axes of a 3D grid (k_plane_pass), 2-CTA clusters
+  int epro = 0;  // 1: epilogue fused with the next iteration's speculative prologue (k_regc_epro)
+  int repair = 0;  // 1: prologue again for rejected right-hand sides (k_regc_repair)
   int64_t rc_tiles = 0;
   size_t rc_smem = 0;
 };
@@ -112,6 +115,8 @@ struct mmx_plan {
   bool pipe = false;           // MMX_PIPE=1: persistent double-buffered prologue/epilogue passes
   bool plane = false;          // plane passes over the two inner axes (3D, 128 x 128 planes, isotropic chi)
   std::vector<PassCfg> plane_passes;  // the 3-pass schedule used when `plane` is set and chi is isotropic
+  bool epro = false;           // fuse each epilogue with the next iteration's prologue (isotropic chi)
+  std::vector<PassCfg> epro_passes;   // [middle passes..., EPI+PRO, repair]; the first PRO runs once per call
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
   size_t l2_window = 0;
@@ -389,8 +394,67 @@ int launch_plane(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s
   return MMX_OK;
 }
 
+template <int C, int N>
+int launch_epro(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  if constexpr (N == 192 || N == 384 || (C == 3 && N > 128)) {
+    return fail(MMX_ERR_ARG, "internal: no fused epilogue kernel for this length");
+  } else {
+    constexpr int PCK = RegCDefault<C, N>::PC_EPI;
+    auto kern = k_regc_epro<C, N, PCK>;
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured_mask & (1 << dev))) {
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+      configured_mask |= (1 << dev);
+    }
+    a.outer = pc.outer;
+    a.inner = pc.inner;
+    a.nrhs = batch;
+    dim3 grid((unsigned)pc.rc_tiles, (unsigned)batch);
+    MMX_CUDA(launch_pass(kern, grid, dim3(RegC<C, N, PCK>::THREADS), pc.rc_smem, s, a));
+    return MMX_OK;
+  }
+}
+
+int sm_count();
+
+template <int C, int N>
+int launch_repair(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  if constexpr (N == 192 || N == 384 || (C == 3 && N > 128)) {
+    return fail(MMX_ERR_ARG, "internal: no repair kernel for this length");
+  } else {
+    constexpr int PCK = RegCDefault<C, N>::PC;
+    auto kern = k_regc_repair<C, N, PCK>;
+    static int configured_mask = 0;
+    static int blocks_per_sm = 1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured_mask & (1 << dev))) {
+      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, RegC<C, N, PCK>::THREADS, pc.rc_smem);
+      if (blocks_per_sm < 1) blocks_per_sm = 1;
+      configured_mask |= (1 << dev);
+    }
+    a.outer = pc.outer;
+    a.inner = pc.inner;
+    a.nrhs = batch;
+    // one wave: it only has work after a rejection
+    const int64_t grid = std::min<int64_t>(pc.rc_tiles, (int64_t)sm_count() * blocks_per_sm);
+    MMX_CUDA(launch_pass(kern, dim3((unsigned)grid), dim3(RegC<C, N, PCK>::THREADS), pc.rc_smem, s, a,
+                         (int)pc.rc_tiles));
+    return MMX_OK;
+  }
+}
+
 template <int C, int CHI, int N>
 int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_t s) {
+  if (pc.epro || pc.repair) {
+    if constexpr (CHI == MMX_CHI_SCALAR) {
+      return pc.epro ? launch_epro<C, N>(pc, a, batch, s) : launch_repair<C, N>(pc, a, batch, s);
+    }
+    return fail(MMX_ERR_ARG, "internal: fused epilogue pass with an anisotropic chi");
+  }
   if (pc.plane) {
     if constexpr (CHI == MMX_CHI_SCALAR && N == mmx_plane::N) {
       switch (pc.ops) {
@@ -544,6 +608,27 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
   return v;
 }
 
+// The per-iteration passes with the epilogue fused to the next iteration's speculative prologue: the middle
+// passes of the plain schedule, then [INV EPI + PRO FWD] and the repair pass (empty when the contiguous axis has no
+// register-staged kernel).  The plain schedule's first pass runs once at the start of every chunk of iterations.
+std::vector<PassCfg> build_epro_passes(const mmx_plan* p) {
+  std::vector<PassCfg> v;
+  if (p->ndim < 2 || p->prec != MMX_C64 || p->force_generic) return v;
+  const std::vector<PassCfg> plain = build_passes(p, false);
+  if (plain.size() < 3 || !plain.front().regc || !plain.back().regc || plain.front().pipe || plain.back().pipe)
+    return v;
+  for (size_t k = 1; k + 1 < plain.size(); ++k) v.push_back(plain[k]);
+  PassCfg epi = plain.back();
+  epi.regc = 0;
+  epi.epro = 1;
+  PassCfg rep = plain.front();
+  rep.regc = 0;
+  rep.repair = 1;
+  v.push_back(epi);
+  v.push_back(rep);
+  return v;
+}
+
 // The 3-pass schedule [PRO FWD ax2 FWD ax1] [FWD G INV ax0] [INV ax1 INV ax2 EPI] of a 3D complex64 grid with
 // 128 x 128 planes (empty when the grid does not qualify).  The axis-0 pass is the one of the 5-pass schedule.
 std::vector<PassCfg> build_plane_passes(const mmx_plan* p) {
@@ -598,6 +683,23 @@ int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kin
   // the accept/reject decision is taken by the last tile of the epilogue pass (no separate launch)
   const bool plane = std::is_same<R, float>::value && p->plane && chi_kind == MMX_CHI_SCALAR &&
                      !p->plane_passes.empty();
+  const bool epro = std::is_same<R, float>::value && !plane && p->epro && chi_kind == MMX_CHI_SCALAR &&
+                    !p->epro_passes.empty();
+  if (epro) {
+    // first prologue of the chunk, then per iteration the middle passes, the fused epilogue + next prologue and
+    // the repair pass
+    a.ax = p->ax[p->iter_passes.front().axis];
+    int rc = dispatch_pass<R>(p->iter_passes.front(), a, p->ncomp, chi_kind, p->batch, s);
+    if (rc != MMX_OK) return rc;
+    for (int it = 0; it < niter; ++it) {
+      for (const PassCfg& pc : p->epro_passes) {
+        a.ax = p->ax[pc.axis];
+        rc = dispatch_pass<R>(pc, a, p->ncomp, chi_kind, p->batch, s);
+        if (rc != MMX_OK) return rc;
+      }
+    }
+    return MMX_OK;
+  }
   const std::vector<PassCfg>& passes = plane ? p->plane_passes : p->iter_passes;
   for (int it = 0; it < niter; ++it) {
     for (const PassCfg& pc : passes) {
@@ -752,6 +854,7 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
   p->iter_passes = build_passes(p, false);
   p->defect_passes = build_passes(p, true);
   p->plane_passes = build_plane_passes(p);
+  p->epro_passes = build_epro_passes(p);
   int64_t maxt = 2048;  // enough partial sums for any tile width (at most one tile per pencil)
   for (int i = 0; i < ndim; ++i) maxt = std::max<int64_t>(maxt, p->N / shape[i]);
   p->partials_len = (int64_t)batch * maxt * 2;
@@ -1008,16 +1111,18 @@ extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const 
 
 extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
   if (!p) return fail(MMX_ERR_ARG, "NULL plan");
-  if (flags & ~15u) return fail(MMX_ERR_ARG, "unknown variant flags");
+  if (flags & ~31u) return fail(MMX_ERR_ARG, "unknown variant flags");
   drop_graphs_of(p);  // captured graphs hold the previous kernels
   p->force_generic = (flags & MMX_VARIANT_GENERIC) != 0;
   p->no_reg = (flags & MMX_VARIANT_SHARED_STAGED) != 0;
   p->pipe = (flags & MMX_VARIANT_PERSISTENT) != 0;
   p->plane = (flags & MMX_VARIANT_PLANE) != 0;
+  p->epro = (flags & MMX_VARIANT_FUSED_EPILOGUE) != 0;
   p->iter_passes = build_passes(p, false);
   p->defect_passes = build_passes(p, true);
   p->plane_passes = build_plane_passes(p);
-  for (const auto* list : {&p->iter_passes, &p->plane_passes})
+  p->epro_passes = build_epro_passes(p);
+  for (const auto* list : {&p->iter_passes, &p->plane_passes, &p->epro_passes})
     for (auto& pc : *list)
       if (2 * (int64_t)p->batch * pc.tiles > p->partials_len) return fail(MMX_ERR_ARG, "internal: partials too small");
   return MMX_OK;
@@ -1026,7 +1131,8 @@ extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
 extern "C" unsigned mmx_plan_get_variant(const mmx_plan* p) {
   if (!p) return 0u;
   return (p->force_generic ? MMX_VARIANT_GENERIC : 0u) | (p->no_reg ? MMX_VARIANT_SHARED_STAGED : 0u) |
-         (p->pipe ? MMX_VARIANT_PERSISTENT : 0u) | (p->plane ? MMX_VARIANT_PLANE : 0u);
+         (p->pipe ? MMX_VARIANT_PERSISTENT : 0u) | (p->plane ? MMX_VARIANT_PLANE : 0u) |
+         (p->epro ? MMX_VARIANT_FUSED_EPILOGUE : 0u);
 }
 
 extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,

@@ -1,0 +1,257 @@
+// Epilogue of iteration k fused with the prologue of iteration k + 1 (contiguous axis, complex64, isotropic chi).
+//
+// Per iteration the unfused schedule streams the field twice through the contiguous-axis passes: the epilogue reads
+// E and writes E' = E + chi (T - E), and the next iteration's prologue reads E' back to form chi E' + s'.  Here the
+// epilogue pass goes on with the values it holds in registers:
+//
+//   k_regc_epro:   inverse FFT of T along the contiguous axis, E' = E + chi (T - E) with the partial norms, then
+//                  x = chi E' + s' and the forward FFT of x, written to T  -- the next iteration's first pass.
+//
+// The forward transform runs the radix plan in reverse order, so its first stage (radix R_last, span 1) reads
+// exactly the positions i + q N / R_last at which the inverse transform's last stage left its outputs: that stage
+// is done in registers, straight after the epilogue, and only the later stages go through shared memory.
+//
+// The prologue is speculative.  chi(alpha) E' + s'(alpha) is the next iteration's input only if the divergence
+// guard accepts E' (the usual case); it is taken at the end of the same pass by the last CTA of each right-hand
+// side.  If it rejects, the next input is chi(alpha') E + s'(alpha') with the old field and alpha' = alpha with its
+// imaginary part raised (solver.py:1090-1094), and k_regc_repair recomputes the prologue pass for that right-hand
+// side.  The repair pass is a grid-stride loop that leaves at once for every right-hand side whose update was
+// accepted (or that is no longer active), so on the common path it costs one short launch.
+#pragma once
+#include "mmx_reg.cuh"
+
+// Stages of `List` on the contiguous layout, the first one at span L; all but the last run in shared memory, the
+// last one (span N / R) writes this thread's row of the destination in global memory.
+template <int DIR, int N, int C, int PC, int L, class List> struct CChainToGlobal;
+template <int DIR, int N, int C, int PC, int L, int R0>
+struct CChainToGlobal<DIR, N, C, PC, L, RegPlanList<R0>> {
+  static __device__ __forceinline__ void run(float2* sm, const float2* tw, float2* __restrict__ grow) {
+    using G = RegC<C, N, PC>;
+    constexpr int TPP = G::TPP, T = N / R0, NB = T / TPP;
+    static_assert(L * R0 == N, "the last stage spans the whole line");
+    static_assert(NB >= 1 && T % TPP == 0, "stage does not split evenly over the threads");
+    const int tid = threadIdx.x;
+    const int ii = tid % TPP;
+    const int row = (tid / TPP) % PC;
+    const int c = tid / (TPP * PC);
+#pragma unroll 1
+    for (int m = 0; m < NB; ++m) {
+      const int i = ii + m * TPP;  // i < T = L, so the twiddle exponent is q i
+      float2 v[R0];
+#pragma unroll
+      for (int q = 0; q < R0; ++q) v[q] = sm[G::idx(c, row, i + q * T)];
+#pragma unroll
+      for (int q = 1; q < R0; ++q) {
+        float2 w = tw[q * i];
+        if (DIR > 0) w = conjc(w);
+        v[q] = v[q] * w;
+      }
+      bfly<float, R0, DIR>(v, tw, N);
+#pragma unroll
+      for (int q = 0; q < R0; ++q) grow[i + q * T] = v[q];
+    }
+  }
+};
+template <int DIR, int N, int C, int PC, int L, int R0, int R1, int... Rs>
+struct CChainToGlobal<DIR, N, C, PC, L, RegPlanList<R0, R1, Rs...>> {
+  static __device__ __forceinline__ void run(float2* sm, const float2* tw, float2* __restrict__ grow) {
+    cstage_smem<DIR, N, C, PC, R0, L>(sm, tw);
+    CChainToGlobal<DIR, N, C, PC, L * R0, RegPlanList<R1, Rs...>>::run(sm, tw, grow);
+  }
+};
+
+// The prologue pass for the tile `tile` of right-hand side b: x = chi(alpha) E + s'(alpha) on the load, forward FFT
+// along the contiguous axis, written to T (the same work as k_regc_pass<C, PRO | FWD>).
+template <int C, int N, int PC>
+__device__ __forceinline__ void regc_pro_tile(const IterArgs<float>& a, int b, int64_t tile, float2* sm,
+                                              const float2* smtw, const ChiCoef<float>& cc, const float2* Ecur) {
+  using G = RegC<C, N, PC>;
+  using PA = RegPlanArgs<typename RegPlan<N>::type>;
+  constexpr int TPP = G::TPP;
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int64_t N3 = a.N;
+  const int64_t fbase = (int64_t)b * C * N3;
+  const int64_t rowbase = (tile * PC + row) * N;
+  constexpr int RAD = PA::R_first;
+  constexpr int T = N / RAD;
+  constexpr int NBT = T / TPP;
+  const float2* __restrict__ eS = Ecur + fbase + c * N3 + rowbase;
+  const float2* __restrict__ sS = a.src + fbase + c * N3 + rowbase;
+  const float2* __restrict__ xS = a.chi + rowbase;
+#pragma unroll 1
+  for (int m = 0; m < NBT; ++m) {
+    const int i = ii + m * TPP;
+    float2 u[RAD];
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) {
+      const int s_ = i + q * T;
+      u[q] = (cc.a * xS[s_] + cc.b) * eS[s_] + cc.s * sS[s_];
+    }
+    bfly<float, RAD, -1>(u, smtw, N);
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[q];
+  }
+  __syncthreads();
+  PA::template mid<-1, N, C, PC>(sm, smtw);
+  constexpr int RL = PA::R_last;
+  constexpr int TL = N / RL;
+  constexpr int NBL = TL / TPP;
+  constexpr int LL = N / RL;
+  float2* __restrict__ tO = a.T + fbase + c * N3 + rowbase;
+#pragma unroll 1
+  for (int m = 0; m < NBL; ++m) {
+    const int i = ii + m * TPP;
+    float2 v[RL];
+#pragma unroll
+    for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+    for (int q = 1; q < RL; ++q) v[q] = v[q] * smtw[q * i];
+    bfly<float, RL, -1>(v, smtw, N);
+#pragma unroll
+    for (int q = 0; q < RL; ++q) tO[i + q * LL] = v[q];
+  }
+}
+
+// The fused pass holds the first forward stage of all its butterflies across a barrier: it is sized for 768 threads
+// per SM (up to 85 registers per thread) rather than the 1024 of the single passes.
+template <int C, int N, int PC> struct EproMinBlocks {
+  static constexpr int T = RegC<C, N, PC>::THREADS;
+  static constexpr int value = 768 / T >= 2 ? 768 / T : 2;
+};
+
+template <int C, int N, int PC>
+__global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, PC>::value))
+    k_regc_epro(IterArgs<float> a) {
+  using G = RegC<C, N, PC>;
+  using Plan = typename RegPlan<N>::type;
+  using PA = RegPlanArgs<Plan>;
+  constexpr int TPP = G::TPP, THREADS = G::THREADS;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * PC * G::PITCH;
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  const int64_t N3 = a.N;
+  const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+  const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
+  if (threadIdx.x == 0) {  // inputs no kernel writes: chi and s'
+    prefetch_l2(a.chi + row0, chunk);
+#pragma unroll
+    for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(a.src + ((int64_t)b * C + cc2) * N3 + row0, chunk);
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
+  const ChiCoef<float> cc = chi_coef<float>(st);
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int64_t fbase = (int64_t)b * C * N3;
+  const int64_t rowbase = ((int64_t)blockIdx.x * PC + row) * N;
+  const int cur = st->cur;
+  const float2* __restrict__ Ecur = cur ? a.E1 : a.E0;
+  float2* __restrict__ Eoth = cur ? a.E0 : a.E1;
+  if (tid == 0) {
+#pragma unroll
+    for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
+  }
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  __syncthreads();
+
+  // inverse transform of T: first stage from global memory, middle stages in shared memory
+  float2* __restrict__ trow = a.T + fbase + c * N3 + rowbase;
+  {
+    constexpr int RAD = PA::R_first;
+    constexpr int T = N / RAD;
+    constexpr int NBT = T / TPP;
+#pragma unroll 1
+    for (int m = 0; m < NBT; ++m) {
+      const int i = ii + m * TPP;
+      float2 u[RAD];
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) u[q] = trow[i + q * T];
+      bfly<float, RAD, +1>(u, smtw, N);
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = u[q];
+    }
+  }
+  __syncthreads();
+  PA::template mid<+1, N, C, PC>(sm, smtw);
+
+  // last inverse stage, epilogue, speculative prologue and the first forward stage, in registers
+  constexpr int RL = PA::R_last;
+  constexpr int TL = N / RL;
+  constexpr int NBL = TL / TPP;
+  constexpr int LL = N / RL;
+  const float2* __restrict__ eS = Ecur + fbase + c * N3 + rowbase;
+  const float2* __restrict__ sS = a.src + fbase + c * N3 + rowbase;
+  const float2* __restrict__ xS = a.chi + rowbase;
+  float2* __restrict__ eO = Eoth + fbase + c * N3 + rowbase;
+  double dd2 = 0.0, en2 = 0.0;
+  float2 xf[NBL][RL];
+#pragma unroll
+  for (int m = 0; m < NBL; ++m) {
+    const int i = ii + m * TPP;
+    float2 v[RL];
+#pragma unroll
+    for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+    for (int q = 1; q < RL; ++q) v[q] = v[q] * conjc(smtw[q * i]);
+    bfly<float, RL, +1>(v, smtw, N);
+#pragma unroll
+    for (int q = 0; q < RL; ++q) {
+      const int s_ = i + q * LL;
+      const float2 e = eS[s_];
+      const float2 x = cc.a * xS[s_] + cc.b;
+      const float2 d = x * (v[q] - e);
+      const float2 en = e + d;
+      eO[s_] = en;
+      dd2 += norm2d(d);
+      en2 += norm2d(en);
+      xf[m][q] = x * en + cc.s * sS[s_];  // next iteration's chi(alpha) E' + s'(alpha), if E' is accepted
+    }
+    bfly<float, RL, -1>(xf[m], smtw, N);  // first forward stage of the reversed plan (span 1)
+  }
+  __syncthreads();  // every thread has read its inputs of the last inverse stage
+#pragma unroll
+  for (int m = 0; m < NBL; ++m) {
+    const int i = ii + m * TPP;
+#pragma unroll
+    for (int q = 0; q < RL; ++q) sm[G::idx(c, row, i * RL + q)] = xf[m][q];
+  }
+  __syncthreads();
+  CChainToGlobal<-1, N, C, PC, RL, typename PlanReverse<typename PlanInit<Plan>::type>::type>::run(sm, smtw, trow);
+  finish_pass_norms(a, b, dd2, en2);
+}
+
+// Prologue pass again for every right-hand side whose last update the divergence guard rejected (the fused pass
+// above computed it from the rejected field).  Grid-stride over the tiles of each such right-hand side.
+template <int C, int N, int PC>
+__global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (RegCMinBlocks<C, OP_PRO | OP_FWD, N, PC>::value))
+    k_regc_repair(IterArgs<float> a, int tiles_per_rhs) {
+  using G = RegC<C, N, PC>;
+  constexpr int THREADS = G::THREADS;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * PC * G::PITCH;
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = threadIdx.x; t < N; t += THREADS) smtw[t] = twg[t];
+  pdl_wait();
+  pdl_trigger();
+  __syncthreads();
+  for (int b = 0; b < a.nrhs; ++b) {
+    const mmx_rhs_state* st = a.st + b;
+    if (!st->active || st->accepted) continue;  // uniform over the CTA
+    const ChiCoef<float> cc = chi_coef<float>(st);
+    const float2* Ecur = st->cur ? a.E1 : a.E0;
+    for (int64_t t = blockIdx.x; t < tiles_per_rhs; t += gridDim.x) {
+      regc_pro_tile<C, N, PC>(a, b, t, sm, smtw, cc, Ecur);
+      __syncthreads();  // the tile's shared memory is free again
+    }
+  }
+}

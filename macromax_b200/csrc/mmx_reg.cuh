@@ -544,10 +544,14 @@ template <int... Rs> struct RegPlanArgs<RegPlanList<Rs...>> {
   };
 };
 
-// Resident CTAs per SM the register budget is sized for: 64 registers per thread, i.e. 1024 threads per SM.
+// Resident CTAs per SM the register budget is sized for: MMX_REGC_THREADS_PER_SM threads per SM (1024 by default,
+// i.e. 64 registers per thread).
+#ifndef MMX_REGC_THREADS_PER_SM
+#define MMX_REGC_THREADS_PER_SM 1024
+#endif
 template <int C, int OPS, int N, int PC_> struct RegCMinBlocks {
   static constexpr int T = RegC<C, N, PC_>::THREADS;
-  static constexpr int value = 1024 / T >= 2 ? 1024 / T : 2;
+  static constexpr int value = MMX_REGC_THREADS_PER_SM / T >= 2 ? MMX_REGC_THREADS_PER_SM / T : 2;
 };
 
 template <int C, int OPS, int N, int PC_>
