@@ -232,7 +232,7 @@ def bench_ours(args, wl, rank, world, local, pg):
     peaks = load_peaks()
     achieved = alg / (ms_per_step / 1e3) / 1e9
     roof = {'bound': 'hbm', 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-            'frac': achieved / peaks['hbm_gbs'], 'traffic': traffic_per_iteration(wl),
+            'frac': achieved / peaks['hbm_gbs'], 'traffic': traffic_per_iteration(wl, tuned['variant'] if tuned else 0),
             'peak_source': peaks['source'],
             'unit_of_launch': f'one iteration = {launches_per_iter} pass kernels (CUDA graph chunks of {chunk})',
             'algorithmic_bytes': alg, 'bytes_per_voxel': alg / nvox}
@@ -254,7 +254,8 @@ def bench_ours(args, wl, rank, world, local, pg):
             'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic (seeded generator)',
             'config': {**config_of(args, wl), 'parallelism': f'replicas x{world}'},
             'roofline': roof, 'cpu_baseline': cpu, 'e2e': e2e, 'clocks': clocks.summary(),
-            'gpu_launches': launches_per_iter * args.steps,
+            'gpu_launches': launches_per_iter * args.steps + (nchunks + rem if fused_epilogue(
+                wl, tuned['variant'] if tuned else 0) else 0),
             'kernel_variant': tuned,
         }
         if secondary is not None:
@@ -262,18 +263,15 @@ def bench_ours(args, wl, rank, world, local, pg):
         print(json.dumps(line), flush=True)
 
 
-def traffic_per_iteration(wl):
-    """DRAM bytes of one iteration from the committed ncu capture of this workload, scaled per voxel (or None)."""
+def traffic_per_iteration(wl, variant=0):
+    """DRAM bytes of one iteration of this workload and kernel variant from the committed ncu capture (or None)."""
     path = os.path.join(ROOT, 'profiles', 'traffic.json')
     try:
         with open(path) as f:
             d = json.load(f)
-        key = f"{wl['name']}"
-        if key in d:
-            return float(d[key]['dram_bytes_per_iteration'])
-    except (OSError, ValueError, KeyError):
-        pass
-    return None
+        return float(d[wl['name']]['variants'][str(int(variant))]['dram_bytes_per_iteration'])
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
 
 
 def run_secondary(args):
@@ -349,12 +347,18 @@ def run_secondary(args):
 
 
 def len_passes(wl, variant=0) -> int:
-    """Pass kernels per iteration: one per axis and direction, or 3 for a 3D grid on the plane passes."""
+    """Pass kernels per iteration: one per axis and direction (2 ndim - 1); 3 for a 3D grid on the plane passes;
+    with the fused epilogue the first pass becomes a repair pass (the same count; one extra prologue per chunk)."""
     d = len(wl['shape'])
     iso = np.asarray(wl['epsilon']).ndim == d
     if d == 3 and (variant or 0) & 8 and tuple(wl['shape'][1:]) == (128, 128) and iso:
         return 3
     return 1 if d == 1 else 2 * d - 1
+
+
+def fused_epilogue(wl, variant=0) -> bool:
+    d = len(wl['shape'])
+    return d > 1 and bool((variant or 0) & 16) and not (variant or 0) & 8 and np.asarray(wl['epsilon']).ndim == d
 
 
 def e2e_solve(wl, dtype):

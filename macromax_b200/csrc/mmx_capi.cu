@@ -439,8 +439,9 @@ int launch_repair(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t 
     a.outer = pc.outer;
     a.inner = pc.inner;
     a.nrhs = batch;
-    // one wave: it only has work after a rejection
-    const int64_t grid = std::min<int64_t>(pc.rc_tiles, (int64_t)sm_count() * blocks_per_sm);
+    // one CTA per SM: it only has work after a rejection, so the common, empty case should launch little
+    (void)blocks_per_sm;
+    const int64_t grid = std::min<int64_t>(pc.rc_tiles, (int64_t)sm_count());
     MMX_CUDA(launch_pass(kern, dim3((unsigned)grid), dim3(RegC<C, N, PCK>::THREADS), pc.rc_smem, s, a,
                          (int)pc.rc_tiles));
     return MMX_OK;
