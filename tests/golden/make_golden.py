@@ -3,7 +3,8 @@ Generate the golden fixtures under ``tests/golden/`` by running the REFERENCE Ma
 
 Run from the repository root, where the reference tree is present:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                     # every fixture
+    python tests/golden/make_golden.py --only-scattering   # the scattering-matrix fixtures only
 
 Every case builds a reference ``macromax.Solution`` on seeded synthetic inputs (``macromax_b200.workloads``) and
 records the preconditioner constants (alpha, beta), the field E after selected iterations, the residue and
@@ -147,8 +148,59 @@ def backend_ops(mm):
     print(f'backend_ops -> {os.path.getsize(path)} B')
 
 
+def scattering_media():
+    """Seeded slab media for the scattering-matrix fixtures: (name, grid shape, step, vectorial, refractive index)."""
+    wavelength = 500e-9
+    rng = np.random.default_rng(13)
+    cases = []
+    for name, shape, vectorial in (('smatrix_1d_scalar', (256,), False),
+                                   ('smatrix_2d_scalar', (256, 7), False),
+                                   ('smatrix_2d_vector', (256, 7), True),
+                                   ('smatrix_3d_scalar', (256, 5, 3), False)):
+        n = np.ones(shape)
+        lo, hi = shape[0] // 2 - 8, shape[0] // 2 + 8
+        ripple = 0.15 * rng.uniform(-1, 1, size=(hi - lo, *shape[1:]))
+        n[lo:hi] = 1.5 + ripple
+        cases.append((name, shape, wavelength / 4, vectorial, n))
+    return wavelength, cases
+
+
+def scattering_cases(mm):
+    """Full scattering matrices of the reference ``ScatteringMatrix`` (complex128, default callback) on small slab
+    media, with the reference test suite's boundary (a 20-wavelength linear absorber on both sides of axis 0), plus
+    outputs of its host-side vector conversions for seeded vectors and fields."""
+    from macromax import matrix
+    from macromax.bound import LinearBound
+    from macromax.utils.ft import Grid
+    wavelength, cases = scattering_media()
+    rng = np.random.default_rng(17)
+    for name, shape, step, vectorial, n in cases:
+        grid = Grid(list(shape), step)
+        thickness = np.zeros((grid.ndim, 1))
+        thickness[0, 0] = 20 * wavelength
+        bound = LinearBound(grid, thickness=thickness, max_extinction_coefficient=0.25)
+        t0 = time.perf_counter()
+        m = matrix.ScatteringMatrix(grid, vectorial=vectorial, vacuum_wavelength=wavelength, refractive_index=n,
+                                    bound=bound, dtype=np.complex128)
+        side = m.shape[0]
+        vec = rng.standard_normal(side) + 1j * rng.standard_normal(side)
+        fld = rng.standard_normal((1 + 2 * vectorial, *shape)) + 1j * rng.standard_normal((1 + 2 * vectorial, *shape))
+        out = dict(shape=np.asarray(shape), step=np.float64(step), wavelength=np.float64(wavelength),
+                   vectorial=np.bool_(vectorial), refractive_index=n, bound_thickness=np.float64(20 * wavelength),
+                   vec=vec, field=fld,
+                   freespace=m.srcvec2freespace(vec), source=m.srcvec2source(vec), detvec=m.detfield2detvec(fld),
+                   S=np.asarray(m).copy())
+        out['seconds'] = np.float64(time.perf_counter() - t0)
+        path = os.path.join(HERE, f'{name}.npz')
+        np.savez_compressed(path, **out)
+        print(f'{name}: side {side}, {out["seconds"]:.1f} s -> {os.path.getsize(path)} B', flush=True)
+
+
 def main():
     mm = import_reference()
+    if '--only-scattering' in sys.argv:
+        scattering_cases(mm)
+        return
     backend_ops(mm)
 
     wl = workloads.disks_2d(n=64, seed=1)
@@ -173,6 +225,7 @@ def main():
         wl['epsilon'].shape) % 1009))
     res['source_checksum'] = np.float64(np.sum(np.abs(wl['source'])))
     save_case('disks2d_256_c128', wl, res, store_inputs=False)
+    scattering_cases(mm)
 
 
 if __name__ == '__main__':
