@@ -150,8 +150,8 @@ class BatchSolution:
 
     @property
     def E(self) -> np.ndarray:
-        f = self.engine.current().cpu().numpy().reshape(self.batch, self.ncomp, *self.grid.shape)
-        return (f / self.wavenumber ** 2).astype(self.dtype)
+        f = self.engine.current() * (1.0 / self.wavenumber ** 2)  # unit conversion on the device
+        return self.engine.to_host(f).reshape(self.batch, self.ncomp, *self.grid.shape).astype(self.dtype, copy=False)
 
     def close(self):
         self.engine.close()

@@ -181,6 +181,19 @@ class IterationEngine:
             chunk = min(chunk * 2, max_chunk)
         return st
 
+    def to_host(self, t: torch.Tensor) -> np.ndarray:
+        """Copy a device tensor to a new host array through a pinned staging buffer (kept for the next call), which
+        runs at full link speed instead of the pageable-copy rate."""
+        nbytes = t.numel() * t.element_size()
+        buf = getattr(self, '_pinned', None)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+            self._pinned = buf
+        view = buf[:nbytes].view(t.dtype).view(t.shape)
+        view.copy_(t.contiguous())
+        torch.cuda.current_stream(t.device).synchronize()
+        return view.numpy().copy()
+
     def close(self):
         if getattr(self, 'plan', None) is not None:
             self.plan.close()

@@ -241,8 +241,8 @@ class Solution:
     @property
     def E(self) -> np.ndarray:
         """solver.py:811-821: the current field divided by k0^2, as a host array."""
-        f = self._engine.current()[0].cpu().numpy().reshape(self._nb_pol, *self._grid.shape)
-        return (f / (self._wavenumber ** 2)).astype(self._dtype)
+        f = self._engine.current()[0] * (1.0 / self._wavenumber ** 2)  # unit conversion on the device
+        return self._engine.to_host(f).reshape(self._nb_pol, *self._grid.shape).astype(self._dtype, copy=False)
 
     @E.setter
     def E(self, E):
