@@ -190,6 +190,17 @@ int mmx_mat3_extremes(mmx_plan* plan, const void* M, int64_t nvox, int mode, dou
                       void* stream);
 
 /*
+ * The alpha objective of the preconditioner for a scalar permittivity (replaces the full-grid host evaluation in
+ * Solution.__prepare_preconditioner, solver.py:392-401): out_dev[0..1] = min, max over the nvox voxels of
+ * (ab^2 - 2 round(x ab)) + p, where xp holds the pairs (x, p) = (Re eps, Re(conj(eps) eps)) in FP64 on the device.
+ * This is the host expression |ab|^2 - (conj(eps) ab + eps conj(ab)) + conj(eps) eps (whose imaginary part is zero for
+ * real ab) evaluated with explicitly rounded operations, so the largest singular value sqrt(max |.|) / |beta| equals
+ * the host's bit for bit.  Uses the plan's scratch.
+ */
+int mmx_scalar_sigma(mmx_plan* plan, const void* xp, int64_t nvox, double ab, double* out_dev, void* stream);
+
+/*
+ * mmx_fftn without a plan and without any device allocation:/*
  * mmx_fftn without a plan and without any device allocation: the same transform as mmx_fftn (forward unscaled,
  * inverse scaled by 1/N) over the `ndim` grid axes `shape` of `nbatch` contiguous fields of the given precision.
  * No counterpart in the reference (which always allocates through its backend).  For callers that must not let a

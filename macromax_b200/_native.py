@@ -43,7 +43,8 @@ assert STATE_DTYPE.itemsize == 112
 EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destroy', 'mmx_plan_set_kvectors',
             'mmx_fftn', 'mmx_norm', 'mmx_iterate', 'mmx_defect', 'mmx_accumulate', 'mmx_adjoint_grad',
             'mmx_pointwise_mul', 'mmx_fftn_noalloc', 'mmx_mat3_extremes', 'mmx_iterate_graph',
-            'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant']
+            'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant',
+            'mmx_scalar_sigma']
 
 _lib = None
 
@@ -79,6 +80,7 @@ def load(path: str | None = None):
         'mmx_adjoint_grad': (i32, [vp, vp, vp, i64, i32, i64, i32, dbl, vp]),
         'mmx_pointwise_mul': (i32, [vp, i32, i32, vp, i32, i32, vp, i64, i32, vp]),
         'mmx_fftn_noalloc': (i32, [i32, ctypes.POINTER(i64), vp, vp, i64, i32, i32, vp]),
+        'mmx_scalar_sigma': (i32, [vp, vp, i64, dbl, vp, vp]),
         'mmx_mat3_extremes': (i32, [vp, vp, i64, i32, dbl, vp, vp]),
         'mmx_iterate_graph': (i32, [vp, vp, vp, vp, i32, vp, vp, i32, vp]),
         'mmx_iterate_graph_prepare': (i32, [vp, vp, vp, vp, i32, vp, vp, i32]),

@@ -1151,6 +1151,19 @@ extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int m
   return MMX_OK;
 }
 
+extern "C" int mmx_scalar_sigma(mmx_plan* p, const void* xp, int64_t nvox, double ab, double* out_dev, void* stream) {
+  if (!p || !xp || !out_dev) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (nvox < 1) return fail(MMX_ERR_ARG, "nvox must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  int blocks = grid_blocks(nvox, 256);
+  if (2 * (int64_t)blocks > p->partials_len) blocks = (int)(p->partials_len / 2);
+  k_scalar_sigma<<<blocks, 256, 0, s>>>((const double2*)xp, nvox, ab, p->partials);
+  MMX_CUDA(cudaGetLastError());
+  k_minmax_final<<<1, 256, 0, s>>>(p->partials, blocks, out_dev);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Allocation-free N-D FFT.
 //

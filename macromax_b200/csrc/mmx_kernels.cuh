@@ -618,6 +618,50 @@ __global__ void k_mat3_extremes(const double2* __restrict__ M, int64_t N, int mo
   }
 }
 
+// Objective of the alpha search for a scalar permittivity (solver.py:392-401, non-magnetic): the host expression
+// |ab|^2 - (conj(eps) ab + eps conj(ab)) + conj(eps) eps has, for real ab, an imaginary part that is exactly zero and
+// the real part (ab^2 - 2 round(x ab)) + p with x = Re eps and p = the host's value of Re(conj(eps) eps).  Evaluated
+// here with explicitly rounded FP64 operations (no fused multiply-add), so min / max over the voxels are those of
+// the host expression bit for bit.  xp: [N] pairs (x, p).  Per-block (min, max) partials as k_mat3_extremes.
+__global__ void k_scalar_sigma(const double2* __restrict__ xp, int64_t N, double ab, double* part) {
+  double vmin = INFINITY, vmax = -INFINITY;
+  const double ab2 = __dmul_rn(ab, ab);
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (int64_t)gridDim.x * blockDim.x) {
+    const double2 q = xp[v];
+    const double t = __dmul_rn(q.x, ab);
+    const double w = __dadd_rn(__dsub_rn(ab2, __dadd_rn(t, t)), q.y);
+    vmin = fmin(vmin, w);
+    vmax = fmax(vmax, w);
+  }
+  __shared__ double smin[32], smax[32];
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    vmin = fmin(vmin, __shfl_down_sync(full, vmin, o));
+    vmax = fmax(vmax, __shfl_down_sync(full, vmax, o));
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    smin[warp] = vmin;
+    smax[warp] = vmax;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    vmin = lane < nw ? smin[lane] : INFINITY;
+    vmax = lane < nw ? smax[lane] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmin = fmin(vmin, __shfl_down_sync(full, vmin, o));
+      vmax = fmax(vmax, __shfl_down_sync(full, vmax, o));
+    }
+    if (lane == 0) {
+      part[2 * blockIdx.x] = vmin;
+      part[2 * blockIdx.x + 1] = vmax;
+    }
+  }
+}
+
 __global__ void k_minmax_final(const double* __restrict__ part, int np, double* out) {
   double vmin = INFINITY, vmax = -INFINITY;
   for (int i = threadIdx.x; i < np; i += blockDim.x) {

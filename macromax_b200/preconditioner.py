@@ -118,12 +118,48 @@ class DeviceSetup:
         return bool(lo < -thr), bool(hi > thr)
 
 
+class ScalarDeviceObjective:
+    """
+    The alpha objective of a scalar permittivity on the GPU (``mmx_scalar_sigma``).  largest_sigma evaluates
+    |ab|^2 - (conj(eps) ab + eps conj(ab)) + conj(eps) eps over the whole grid for every Nelder-Mead step; for real ab
+    its imaginary part is exactly zero and its real part is (ab^2 - 2 round(Re(eps) ab)) + Re(conj(eps) eps).  The last
+    term is taken from numpy once, and the device evaluates the rest with explicitly rounded FP64 operations, so every
+    objective value -- and hence the simplex path and alpha -- is the host's bit for bit.
+    """
+
+    def __init__(self, eps_field: np.ndarray, device=None):
+        import ctypes
+        import torch
+        from . import _native as nat
+        self._nat, self._ctypes, self._torch = nat, ctypes, torch
+        e = np.ravel(eps_field[0, 0])
+        self.nvox = e.size
+        xp = np.empty((self.nvox, 2), dtype=np.float64)
+        xp[:, 0] = e.real
+        xp[:, 1] = (np.conj(e) * e).real
+        dev = torch.device(device if device is not None else 'cuda')
+        self.xp = torch.from_numpy(xp).to(dev)
+        self.out = torch.zeros(2, dtype=torch.float64, device=dev)
+        with torch.cuda.device(dev):
+            self.plan = nat.Plan((8,), 1, 1, nat.MMX_C128)
+
+    def __call__(self, alpha_real, beta: float) -> float:
+        ab = float(np.ravel(np.real(alpha_real))[0]) * beta
+        c = self._ctypes
+        s = self._torch.cuda.current_stream().cuda_stream
+        self._nat.call('mmx_scalar_sigma', self.plan.handle, c.c_void_p(self.xp.data_ptr()), self.nvox, float(ab),
+                       c.c_void_p(self.out.data_ptr()), c.c_void_p(s) if s else None)
+        lo, hi = self.out.cpu().numpy()
+        return max(abs(float(lo)), abs(float(hi))) ** 0.5 / abs(beta)
+
+
 def prepare(eps_field: np.ndarray, thickness: np.ndarray, wavenumber: float, eps_dtype: float,
             mu: complex = 1.0, objective=None, device_setup: bool = False, device=None) -> Preconditioner:
     """
     eps_field: permittivity as a matrix field [1|3, 1|3, *grid] (boundary susceptibility included).
     objective: optional callable alpha_r -> sigma replacing ``largest_sigma``.
-    device_setup: evaluate the anisotropic objective and the gain/loss test on the GPU (DeviceSetup).
+    device_setup: evaluate the objective on the GPU: the anisotropic objective and gain/loss test (DeviceSetup), and
+    the scalar objective for grids of 65536 voxels or more (ScalarDeviceObjective, the same values as the host's).
     """
     beta = float(np.real(1.0 / mu))  # solver.py:446
     dev = None
@@ -137,6 +173,11 @@ def prepare(eps_field: np.ndarray, thickness: np.ndarray, wavenumber: float, eps
     if objective is None and dev is not None:
         def objective(ar):
             return dev.sigma(ar, beta)
+    if objective is None and device_setup and _is_scalar_field(eps_field) and eps_field[0, 0].size >= (1 << 16):
+        scalar_dev = ScalarDeviceObjective(eps_field, device)
+
+        def objective(ar):
+            return scalar_dev(ar, beta)
     if objective is None:
         def objective(ar):
             return largest_sigma(ar, beta, eps_field)

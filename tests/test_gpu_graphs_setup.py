@@ -81,3 +81,27 @@ def test_device_gain_loss_flags_on_lossy_and_gain_media():
     both[2, 2, 3, 3] -= 0.05j
     for m in (base, lossy, gain, both):
         assert pc.DeviceSetup(m).gain_loss(e) == (pc.has_gain(m, e), pc.has_gain(-m, e))
+
+
+@pytest.mark.parametrize('name', ['disks2d_256', 'spheres3d_64', 'gain2d'])
+def test_scalar_device_objective_is_bitwise_host(name):
+    """The scalar alpha objective on the device equals the host expression bit for bit, so the Nelder-Mead path and
+    alpha are unchanged (solver.py:392-401, 425-461)."""
+    from macromax_b200 import preconditioner as pc
+    from macromax_b200 import workloads
+    if name == 'disks2d_256':
+        eps = workloads.disks_2d(n=256)['epsilon']
+    elif name == 'spheres3d_64':
+        eps = workloads.spheres_3d(n=64, nb_spheres=40)['epsilon']
+    else:
+        eps = workloads.disks_2d(n=256, seed=7)['epsilon'].copy()
+        eps[100:140, 100:140] = 2.0 - 0.4j  # gain: the alpha search is conjugated afterwards
+    eps = np.asarray(eps, dtype=np.complex128)[None, None]
+    obj = pc.ScalarDeviceObjective(eps)
+    for ar in (0.0, 1.0, 0.37, 1.9999, -3.25, 12.5):
+        for beta in (1.0, 0.5):
+            assert obj(ar, beta) == pc.largest_sigma(ar, beta, eps)
+    thickness = np.full((eps.ndim - 2, 2), 2e-6)
+    host = pc.prepare(eps, thickness, 2 * np.pi / 500e-9, float(np.finfo(np.float32).eps), device_setup=False)
+    devp = pc.prepare(eps, thickness, 2 * np.pi / 500e-9, float(np.finfo(np.float32).eps), device_setup=True)
+    assert devp.alpha == host.alpha and devp.transpose == host.transpose
