@@ -276,8 +276,9 @@ def traffic_per_iteration(wl, variant=0):
 
 def run_secondary(args):
     """
-    The batched forms of the metric on smaller instances of the other configurations (seconds, device-timed by
-    synchronisation around whole solves):
+    The other configurations (seconds, device-timed by synchronisation around whole solves):
+      - 2D scalar 256^2 disks in complex128 to 1e-6 or 500 iterations, set-up included;
+      - 3D anisotropic 192^3 Voronoi grains, complex64 inner iterations with FP64 defect correction, to 1e-8;
       - batched mixed precision (2D scalar slab, 512^2 grid, 256 plane-wave sources) to residue 1e-8, against the
         plain complex64 per-source loop (one Solution per source, to 1e-5: single precision cannot reach 1e-8),
         measured on 4 sources and scaled to 256;
@@ -319,6 +320,40 @@ def run_secondary(args):
         'plain_c64_loop_to_1e-5_s (4-source sample x 64)': plain_256, 'plain_iterations_per_source': its / 4,
         'speedup_vs_plain_loop': plain_256 / mixed_s,
         'voxel_iterations_per_s': 256 * 512 * 512 * inner / mixed_s}
+    # 2D scalar Helmholtz, complex128 (the reference NumPy backend's configuration): 256^2 disks to 1e-6 or 500
+    # iterations, including the set-up, second of two runs
+    wl = workloads.disks_2d(n=256)
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    for rep in range(2):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                       source_distribution=wl['source'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                       dtype=np.complex128)
+        sol.solve(None, rtol=1e-6, maxiter=500)
+        E = sol.E
+        b = time.perf_counter()
+        sol._engine.close()
+    out['disks2d_256_c128'] = {'time_to_solution_s (set-up included)': b - a, 'iterations': int(sol.iteration),
+                               'residue': float(sol.residue), 'voxel_iterations_per_s': 256 ** 2 * sol.iteration / (b - a)}
+    del E
+    # 3D anisotropic vector Maxwell, 192^3 Voronoi grains: complex64 inner iterations + FP64 defect correction to 1e-8
+    wl = workloads.voronoi_3d(n=192)
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    ms = MixedSolution(grid, wl['source'], wl['epsilon'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                       vacuum_wavelength=wl['wavelength'])
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    ms.solve(rtol=1e-8)
+    torch.cuda.synchronize()
+    c = time.perf_counter()
+    out['anisotropic_voronoi3d_192_mixed'] = {
+        'setup_s': b - a, 'time_to_1e-8_s': c - b, 'max_residue': float(ms.residues.max()),
+        'inner_iterations': ms.total_inner_iterations, 'outer_steps': len(ms.outer_residues),
+        'voxel_iterations_per_s': 192 ** 3 * ms.total_inner_iterations / (c - b)}
+    ms.close()
     wl = workloads.design_3d(n=128, nb_sources=32)
     grid = Grid(shape=wl['shape'], step=wl['step'])
     k0 = 2 * np.pi / wl['wavelength']

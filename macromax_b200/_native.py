@@ -53,6 +53,14 @@ class NativeError(RuntimeError):
     pass
 
 
+def device_ptr(t) -> ctypes.c_void_p:
+    """Device address of a tensor for the C ABI, whose buffers are dense and row-major: a strided view would be read
+    in the wrong order, so it is refused."""
+    if not t.is_contiguous():
+        raise ValueError(f'the C ABI needs contiguous tensors (shape {tuple(t.shape)}, strides {t.stride()})')
+    return ctypes.c_void_p(t.data_ptr())
+
+
 def load(path: str | None = None):
     """Load (once) and return the ctypes library handle; ImportError if the library cannot be loaded."""
     global _lib

@@ -29,7 +29,7 @@ from .grid import Grid
 
 
 def _ptr(t):
-    return ctypes.c_void_p(t.data_ptr())
+    return nat.device_ptr(t)
 
 
 def _now() -> float:

@@ -36,8 +36,7 @@ def ctypes_void(v):
 
 
 def _ptr(t: torch.Tensor):
-    import ctypes
-    return ctypes.c_void_p(t.data_ptr())
+    return nat.device_ptr(t)
 
 
 class IterationEngine:

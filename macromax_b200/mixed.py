@@ -27,7 +27,7 @@ from .grid import Grid
 
 
 def _ptr(t):
-    return ctypes.c_void_p(t.data_ptr())
+    return nat.device_ptr(t)
 
 
 def _stream():
@@ -58,9 +58,10 @@ class MixedSolution:
             self.plan64.set_kvectors([np.asarray(k, dtype=np.float64).ravel() for k in (grid * self.wavenumber).k])
             m = pre.chi.shape[0] * pre.chi.shape[1]
             chi = np.broadcast_to(pre.chi, (pre.chi.shape[0], pre.chi.shape[1], *grid.shape)).reshape(m, N)
-            self.chi64 = torch.from_numpy(np.array(chi, dtype=np.complex128)).to(self.device)
+            # C order explicitly: a permittivity built as a strided view reshapes to a strided view too
+            self.chi64 = torch.from_numpy(np.ascontiguousarray(chi, dtype=np.complex128)).to(self.device)
             s0 = src.reshape(self.batch, self.ncomp, N) * (1.0j / pre.alpha.imag / pre.beta)
-            self.src64 = torch.from_numpy(np.array(s0, dtype=np.complex128)).to(self.device)
+            self.src64 = torch.from_numpy(np.ascontiguousarray(s0, dtype=np.complex128)).to(self.device)
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
             self._norm = torch.zeros(1, dtype=torch.float64, device=self.device)
         self.outer_residues = []

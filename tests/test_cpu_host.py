@@ -107,3 +107,12 @@ def test_solution_fails_loudly_without_gpu():
     grid = Grid(shape=(16,), step=0.1)
     with pytest.raises(ImportError):
         Solution(grid, vacuum_wavelength=1.0, source_distribution=np.ones((1, 16)), epsilon=np.ones(16))
+
+
+def test_device_ptr_refuses_strided_tensors():
+    import torch
+    from macromax_b200 import _native as nat
+    t = torch.zeros((4, 6), dtype=torch.complex64)
+    assert nat.device_ptr(t).value == t.data_ptr()
+    with pytest.raises(ValueError):
+        nat.device_ptr(t.t())

@@ -48,3 +48,41 @@ def test_plain_complex64_stalls_above_1e8():
                    dtype=np.complex64)
     sol.solve(None, rtol=1e-8, maxiter=1500)
     assert sol.residue > 1e-8
+
+
+def test_mixed_anisotropic_strided_permittivity():
+    """A permittivity built as a strided view (the Voronoi generator's moveaxis): the FP64 defect still reads chi in
+    row-major order -- it equals the oracle's s' + chi x - G^{-1} x -- and the solve reaches 1e-8."""
+    import ctypes
+    import torch
+    from macromax_b200 import Bound, Grid, workloads
+    from macromax_b200 import _native as nat
+    from macromax_b200.mixed import MixedSolution
+    from oracle import mmoracle as mo
+    wl = workloads.voronoi_3d(n=32, nb_grains=8)
+    assert not np.asarray(wl['epsilon']).flags['C_CONTIGUOUS']
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    ms = MixedSolution(grid, wl['source'], wl['epsilon'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                       vacuum_wavelength=wl['wavelength'])
+    eng = ms.inner.engine
+    ref = mo.from_workload(wl, np.complex128)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((3, *wl['shape'])) + 1j * rng.standard_normal((3, *wl['shape']))
+    ms.x.copy_(torch.from_numpy(x.reshape(1, 3, -1)).to(ms.x.device))
+    st = eng.read_state()
+    st['active'] = 1
+    eng.write_state(st)
+    s = torch.cuda.current_stream().cuda_stream
+    nat.call('mmx_defect', ms.plan64.handle, nat.device_ptr(ms.x), nat.device_ptr(ms.chi64), eng.chi_kind,
+             nat.device_ptr(ms.src64), nat.device_ptr(eng.state), nat.device_ptr(eng.sources),
+             ctypes.c_void_p(s) if s else None)
+    dev = eng.sources.cpu().numpy().reshape(3, 1, *wl['shape'])
+    xo = x[:, None]
+    host = ref.source_normalized + ref.chi_op(xo) - mo.inverse_green_op(ref, xo)
+    assert rel(dev, host) < 1e-6  # the stored defect is complex64
+    ms.close()
+    ms = MixedSolution(grid, wl['source'], wl['epsilon'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                       vacuum_wavelength=wl['wavelength'])
+    ms.solve(rtol=1e-8)
+    assert ms.converged.all() and ms.residues.max() < 1e-8
+    ms.close()
