@@ -351,3 +351,147 @@ def inverse_green_op(sol: OracleSolution, x):
 
 def num_threads() -> int:
     return os.cpu_count() or 1
+
+
+class MagneticOracleSolution(OracleSolution):
+    """
+    Restatement of ``Solution`` for magnetic and bi-(an)isotropic media: the magnetic branch of
+    ``__prepare_preconditioner`` (solver.py:270-493: alpha and beta by a 2-parameter Nelder-Mead search over the sum of
+    the largest singular values of the E-E, E-H, H-E and H-H blocks), the magnetic ``chi_op`` (solver.py:531-552:
+    chi_EE E + chi_HE D E + D(chi_EH E + chi_HH D E), D the spectral curl of backend/__init__.py:472-509) and the
+    rescaling of all four blocks in ``__update_operators`` (solver.py:514-528).  Fields are vectorial.
+    """
+
+    def __init__(self, shape, step, wavelength, epsilon, source, xi=0.0, zeta=0.0, mu=1.0, bound_thickness=0.0,
+                 dtype=np.complex128, initial_field=0.0):
+        self._material = (xi, zeta, mu)
+        super().__init__(shape, step, wavelength, epsilon, source, bound_thickness=bound_thickness, dtype=dtype,
+                         initial_field=initial_field)
+
+    # backend-like helpers for matrix fields with scalar fields as multiples of the 3x3 identity
+    def _eye(self):
+        return np.eye(3).reshape(3, 3, *([1] * self.ndim)).astype(self.dtype)
+
+    @staticmethod
+    def _is_scalar(a):
+        a = np.asarray(a)
+        return a.ndim == 0 or (a.shape[0] == 1 and (a.ndim == 1 or a.shape[1] == 1))
+
+    def _field(self, a):
+        return to_matrix_field(np.asarray(a, dtype=self.dtype), self.ndim)
+
+    def _subtract(self, left, right):
+        """backend/__init__.py:397-413: a scalar term becomes a multiple of the identity next to a matrix."""
+        if not self._is_scalar(left) or not self._is_scalar(right):
+            if self._is_scalar(left):
+                left = self._eye() * self._field(left)
+            if self._is_scalar(right):
+                right = self._eye() * self._field(right)
+        return left - right
+
+    def _inv(self, m):
+        """backend/numpy.py:135-170 (ldivide with numerator 1)."""
+        m = self._field(m)
+        if self._is_scalar(m):
+            return np.asarray(self._field(1.0), dtype=self.dtype) / m
+        moved = np.moveaxis(m, (0, 1), (-2, -1))
+        return np.moveaxis(np.linalg.inv(moved), (-2, -1), (0, 1))
+
+    def _largest_eigenvalue(self, a):
+        return largest_hermitian_eigenvalue(a, self.ndim)
+
+    def _prepare(self, epsilon, source):
+        if not self.vectorial:
+            raise ValueError('magnetic media need a vector field')
+        xi, zeta, mu = self._material
+        eps = self._field(epsilon)
+        xi = self._field(xi)
+        zeta = self._field(zeta)
+        mu = self._field(mu)
+        gain = any(has_gain(a, self.ndim, self.eps_dtype) for a in (eps, xi, zeta, mu))
+        loss = any(has_gain(-a, self.ndim, self.eps_dtype) for a in (eps, xi, zeta, mu))
+        self.transpose = gain and not loss  # not applied to alpha in the magnetic branch (solver.py:421-442)
+        mu_inv = self._inv(mu)
+        mu_inv_t = adjoint(mu_inv)
+        mu_inv2 = pointwise_mul(mu_inv_t, mu_inv)
+
+        def chi_hh(beta_):
+            return self._subtract(1.0, mu_inv / beta_)
+
+        def chi_hh_beta2(beta_):
+            return mu_inv2 + self._subtract(np.abs(beta_) ** 2, mu_inv_t * beta_ + mu_inv * np.conj(beta_))
+
+        def sigma_hh(beta_):
+            return self._largest_eigenvalue(chi_hh_beta2(beta_)) ** 0.5 / abs(beta_)
+
+        chi_eh_beta = -1.0j * pointwise_mul(xi, mu_inv)
+        chi_he_beta = 1.0j * pointwise_mul(mu_inv, zeta)
+        e_xz = self._subtract(eps, pointwise_mul(xi, -1.0j * chi_he_beta))
+
+        def delta_ee_beta2(alpha_, beta_):
+            ab = np.asarray(np.real(alpha_) * beta_, dtype=self.dtype)
+            res = adjoint(e_xz) * ab
+            res = res + e_xz * np.conj(ab)
+            res = self._subtract(np.abs(ab) ** 2, res)
+            return res + pointwise_mul(adjoint(e_xz), e_xz)
+
+        def sigma_ee(alpha_, beta_):
+            return float(self._largest_eigenvalue(delta_ee_beta2(alpha_, beta_))) ** 0.5 / abs(float(beta_))
+
+        sigma_d = float(np.linalg.norm(2.0 * np.pi / (2.0 * self.step))) / self.wavenumber
+        sigma_he = self._largest_eigenvalue(pointwise_mul(adjoint(chi_he_beta), chi_he_beta)) ** 0.5
+        sigma_eh = self._largest_eigenvalue(pointwise_mul(adjoint(chi_eh_beta), chi_eh_beta)) ** 0.5
+
+        def singular_value_sum(eta_, beta_):
+            return sigma_d ** 2 * sigma_hh(beta_) + sigma_d * (sigma_eh + sigma_he) / np.abs(beta_) \
+                + sigma_ee(eta_, beta_)
+
+        def target(vec):
+            beta_ = vec[1] ** 2  # positive
+            return singular_value_sum(vec[0], beta_) * beta_ + np.maximum(0.0, beta_ - 1e-3) ** 2
+
+        vec = scipy.optimize.fmin(target, [0, 1], initial_simplex=[[0, 1], [1, 1], [0, 0.9]], disp=False,
+                                  full_output=False, ftol=0.01, xtol=0.01, maxiter=100, maxfun=200)
+        self.beta = float(vec[1] ** 2)
+        alpha = vec[0] + 1.0j * singular_value_sum(vec[0], self.beta)
+        alpha = self._increase_bias(complex(alpha))
+        self.alpha = alpha
+        s = 1.0j / alpha.imag / self.beta
+        self.chi_eh = np.asarray(chi_eh_beta * s, dtype=self.dtype)
+        self.chi_he = np.asarray(chi_he_beta * s, dtype=self.dtype)
+        self.chi_hh = np.asarray(chi_hh(self.beta) * (1.0j / alpha.imag), dtype=self.dtype)
+        chi = e_xz * s
+        if chi.shape[0] == 1:
+            chi = chi - alpha * 1.0j / alpha.imag
+        else:
+            chi = chi - self._eye() * (alpha * 1.0j / alpha.imag)
+        self.chi = np.asarray(chi, dtype=self.dtype)
+        self.epsilon_field = eps
+        src = to_matrix_field(np.asarray(source, dtype=self.dtype), self.ndim)
+        if src.shape[0] != self.nb_pol:
+            src = np.broadcast_to(src, (self.nb_pol, *src.shape[1:]))
+        self.source_normalized = np.asarray(src * s, dtype=self.dtype)
+        self.previous_update_norm = np.inf
+        self._update_operators(alpha)
+
+    def _update_operators(self, alpha):
+        old = getattr(self, 'alpha', alpha)
+        if hasattr(self, 'chi_eh'):
+            f = old.imag / alpha.imag
+            self.chi_eh = np.asarray(self.chi_eh * f, dtype=self.dtype)
+            self.chi_he = np.asarray(self.chi_he * f, dtype=self.dtype)
+            self.chi_hh = np.asarray(self.chi_hh * f, dtype=self.dtype)
+        super()._update_operators(alpha)
+
+    def curl(self, F):
+        """D: the spectral curl i k x F of the k0-scaled grid (backend/__init__.py:472-509)."""
+        return np.asarray(ifftn(curl_ft(np.asarray(fftn(F, self.ft_axes)), self.ks), self.ft_axes), dtype=self.dtype)
+
+    def chi_op(self, x):
+        """solver.py:531-552: chi_EE x + chi_HE D x + D(chi_EH x + chi_HH D x)."""
+        chi_e = pointwise_mul(self.chi, x)
+        chi_h = pointwise_mul(self.chi_eh, x)
+        dx = self.curl(x)
+        chi_e = chi_e + pointwise_mul(self.chi_he, dx)
+        chi_h = chi_h + pointwise_mul(self.chi_hh, dx)
+        return np.asarray(chi_e + self.curl(chi_h), dtype=self.dtype)

@@ -5,6 +5,7 @@ Run from the repository root, where the reference tree is present:
 
     python tests/golden/make_golden.py                     # every fixture
     python tests/golden/make_golden.py --only-scattering   # the scattering-matrix fixtures only
+    python tests/golden/make_golden.py --only-magnetic     # the magnetic-media fixtures only
 
 Every case builds a reference ``macromax.Solution`` on seeded synthetic inputs (``macromax_b200.workloads``) and
 records the preconditioner constants (alpha, beta), the field E after selected iterations, the residue and
@@ -196,8 +197,79 @@ def scattering_cases(mm):
         print(f'{name}: side {side}, {out["seconds"]:.1f} s -> {os.path.getsize(path)} B', flush=True)
 
 
+def magnetic_media():
+    """Seeded magnetic media for the magnetic-iteration fixtures: (name, shape, epsilon, xi, zeta, mu, source)."""
+    wavelength, step = 500e-9, 500e-9 / 4
+    cases = []
+    # a negative-index plate (epsilon = mu = -|n|, the conversion of solver.py:227-236 for n = -1.5) in 2D
+    n = 48
+    x0 = (np.arange(n) - n // 2)[:, None] * step
+    plate = np.abs(x0) < 8 * step
+    ramp = workloads.ramp_extinction((n, n), 8, 0.5)
+    eps = np.where(plate, -2.25, 1.0) + 0.01j + 1j * ramp
+    mu = np.where(plate, -1.0, 1.0) + 0.01j + np.zeros((n, n))
+    src = np.zeros((3, n, n), dtype=np.complex128)
+    g = np.exp(-0.5 * ((np.arange(n) - n / 3) / 6.0) ** 2)
+    src[1, n - 10, :] = g
+    src[2, n - 10, :] = 1j * g
+    cases.append(('magnetic2d_48_c128', (n, n), eps, 0.0, 0.0, mu, src))
+    # a lossy chiral sphere (bi-isotropic: xi = -i kappa, zeta = i kappa) in 3D
+    n = 16
+    grid = np.ogrid[0:n, 0:n, 0:n]
+    r2 = sum((gg - n / 2 + 0.5) ** 2 for gg in grid)
+    sphere = r2 <= 4.5 ** 2
+    ramp = workloads.ramp_extinction((n, n, n), 3, 0.5)
+    eps = np.where(sphere, 2.0 + 0.1j, 1.0) + 1j * ramp
+    mu = np.where(sphere, 1.2 + 0.05j, 1.0) + np.zeros((n, n, n))
+    kappa = np.where(sphere, 0.1, 0.0)
+    xi, zeta = -1j * kappa, 1j * kappa
+    src = np.zeros((3, n, n, n), dtype=np.complex128)
+    src[0, :, :, 4] = np.outer(np.exp(-0.5 * ((np.arange(n) - n / 2) / 4.0) ** 2),
+                               np.exp(-0.5 * ((np.arange(n) - n / 2) / 4.0) ** 2))
+    cases.append(('chiral3d_16_c128', (n, n, n), eps, xi, zeta, mu, src))
+    return wavelength, step, cases
+
+
+def magnetic_cases(mm):
+    """Iterates of the reference Solution on magnetic media (complex128, NumPy backend): alpha, beta, fields after
+    selected iterations and the update-norm history."""
+    from macromax.bound import Bound
+    from macromax.utils.ft import Grid
+    wavelength, step, cases = magnetic_media()
+    for name, shape, eps, xi, zeta, mu, src in cases:
+        grid = Grid(list(shape), step)
+        bound = Bound(grid, thickness=2 * step)
+        t0 = time.perf_counter()
+        sol = mm.Solution(grid, vacuum_wavelength=wavelength, epsilon=eps, xi=xi, zeta=zeta, mu=mu,
+                          source_distribution=src, bound=bound, dtype=np.complex128)
+        out = dict(shape=np.asarray(shape), step=np.float64(step), wavelength=np.float64(wavelength), epsilon=eps,
+                   xi=np.asarray(xi), zeta=np.asarray(zeta), mu=np.asarray(mu), source=src,
+                   bound_thickness=np.float64(2 * step), alpha0=np.complex128(sol._Solution__alpha),
+                   beta=np.float64(np.real(sol._Solution__beta)))
+        norms, fields = [], {}
+        for s in sol:
+            norms.append(s.previous_update_norm)
+            if s.iteration in (1, 5, 60):
+                fields[s.iteration] = s.E.copy()
+            if s.iteration >= 60:
+                break
+        out['update_norms'] = np.asarray(norms)
+        out['record'] = np.asarray(sorted(fields))
+        for it, f in fields.items():
+            out[f'E{it}'] = f
+        out['alpha_final'] = np.complex128(sol._Solution__alpha)
+        out['seconds'] = np.float64(time.perf_counter() - t0)
+        path = os.path.join(HERE, f'{name}.npz')
+        np.savez_compressed(path, **out)
+        print(f'{name}: alpha {out["alpha0"]:.6g} beta {out["beta"]:.6g}, {out["seconds"]:.1f} s -> '
+              f'{os.path.getsize(path)} B', flush=True)
+
+
 def main():
     mm = import_reference()
+    if '--only-magnetic' in sys.argv:
+        magnetic_cases(mm)
+        return
     if '--only-scattering' in sys.argv:
         scattering_cases(mm)
         return
@@ -226,6 +298,7 @@ def main():
     res['source_checksum'] = np.float64(np.sum(np.abs(wl['source'])))
     save_case('disks2d_256_c128', wl, res, store_inputs=False)
     scattering_cases(mm)
+    magnetic_cases(mm)
 
 
 if __name__ == '__main__':

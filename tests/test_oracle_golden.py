@@ -90,3 +90,20 @@ def test_full_size_disks_first_iterate():
     for it in (1, 20):
         ref = z[f'E_{it}']
         assert np.linalg.norm(rec[it] - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize('name', ['magnetic2d_48_c128', 'chiral3d_16_c128'])
+def test_magnetic_oracle_matches_reference(name):
+    """Magnetic / bi-isotropic media: the restated 2-parameter preconditioner gives the reference's alpha and beta
+    exactly, and the iterates (chi_op with spectral curls) agree to 1e-13 (fixtures from make_golden.py)."""
+    z = load_golden(name)
+    ref = mo.MagneticOracleSolution(tuple(int(s) for s in z['shape']), float(z['step']), float(z['wavelength']),
+                                    z['epsilon'], z['source'], xi=z['xi'], zeta=z['zeta'], mu=z['mu'],
+                                    bound_thickness=float(z['bound_thickness']))
+    assert ref.alpha == complex(z['alpha0']) and ref.beta == float(z['beta'])
+    record = tuple(int(r) for r in z['record'])
+    rec = ref.solve(rtol=0, maxiter=max(record), record=record)
+    for it in record:
+        g = z[f'E{it}']
+        assert np.linalg.norm(rec[it] - g) <= 1e-13 * np.linalg.norm(g), it
+    assert ref.alpha == complex(z['alpha_final'])
