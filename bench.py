@@ -279,6 +279,7 @@ def run_secondary(args):
     The other configurations (seconds, device-timed by synchronisation around whole solves):
       - 2D scalar 256^2 disks in complex128 to 1e-6 or 500 iterations, set-up included;
       - 3D anisotropic 192^3 Voronoi grains, complex64 inner iterations with FP64 defect correction, to 1e-8;
+      - a magnetic medium (the reference test suite's negative-index plate, 128^2) to residue 1e-3;
       - batched mixed precision (2D scalar slab, 512^2 grid, 256 plane-wave sources) to residue 1e-8, against the
         plain complex64 per-source loop (one Solution per source, to 1e-5: single precision cannot reach 1e-8),
         measured on 4 sources and scaled to 256;
@@ -354,6 +355,29 @@ def run_secondary(args):
         'inner_iterations': ms.total_inner_iterations, 'outer_steps': len(ms.outer_residues),
         'voxel_iterations_per_s': 192 ** 3 * ms.total_inner_iterations / (c - b)}
     ms.close()
+    # magnetic medium: the reference test suite's negative-index plate (128^2, complex64) to residue 1e-3
+    from macromax_b200 import LinearBound, solve
+    wavelength, k0 = 500e-9, 2 * np.pi / 500e-9
+    grid = Grid(shape=(128, 128), step=wavelength / 4)
+    rz = np.array([[np.cos(np.pi / 6), -np.sin(np.pi / 6), 0], [np.sin(np.pi / 6), np.cos(np.pi / 6), 0], [0, 0, 1]])
+    kin = rz * k0 @ np.array([1, 0, 0])
+    cur = np.exp(1j * (kin[0] * grid[0] + kin[1] * grid[1]))
+    sp = grid.shape[0] - int(2e-6 / grid.step[0])
+    cur[:sp, :] = 0
+    cur[sp + 1:, :] = 0
+    cur = cur * np.exp(-0.5 * ((grid[1] - grid[1].ravel()[grid.shape[0] // 3]) / 2.5e-6) ** 2)
+    cur = cur[np.newaxis] * (rz @ np.array([0, 1, 1j]) / np.sqrt(2))[:, np.newaxis, np.newaxis]
+    n = 1 + (-1.5 - 1) * np.ones(grid[1].shape) * (np.abs(grid[0]) < 2.5e-6)
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    sol = solve(grid, vacuum_wavelength=wavelength, current_density=cur, refractive_index=n,
+                bound=LinearBound(grid, thickness=2e-6, max_extinction_coefficient=0.5),
+                callback=lambda s: s.iteration < 1e4 and s.residue > 1e-3, dtype=np.complex64)
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    out['magnetic_negative_index_plate_128'] = {'time_to_1e-3_s (set-up included)': b - a,
+                                                'iterations': int(sol.iteration), 'residue': float(sol.residue)}
+    sol.close()
     wl = workloads.design_3d(n=128, nb_sources=32)
     grid = Grid(shape=wl['shape'], step=wl['step'])
     k0 = 2 * np.pi / wl['wavelength']

@@ -190,6 +190,28 @@ int mmx_mat3_extremes(mmx_plan* plan, const void* M, int64_t nvox, int mode, dou
                       void* stream);
 
 /*
+ * Magnetic and bi-(an)isotropic media (solver.py:531-552): the susceptibility operator
+ * chi(x) = chi_EE x + chi_HE D x + D(chi_EH x + chi_HH D x), D = the spectral curl (backend/__init__.py:472-509), is
+ * composed on the host from mmx_fftn and these kernels.  Fields are [3][N] in the plan's precision; k are the plan's
+ * k-vectors (mmx_plan_set_kvectors, k0-scaled grid).
+ *   mmx_curl_ft:  out = i k x F for a spectrum F (not in place).            Replaces BackEnd.curl_ft (:483-509).
+ *   mmx_green_ft: F <- g (F - P_L F) + (i alpha_i / alpha) P_L F in place,   Replaces g_ft_op (solver.py:571-577).
+ *                 g = -i alpha_i / (|k|^2 - alpha); no 1/N (the inverse mmx_fftn scales).
+ *   mmx_chi_mix:  u = (a chi_EE0 + b I) x + f_HE chi_HE0 d, w = f_EH chi_EH0 x + f_HH chi_HH0 d per voxel, the four
+ *                 blocks [9][N] (row-major 3x3) stored at alpha0; coef = the complex pairs (a, b, f_EH, f_HE, f_HH)
+ *                 in FP64 (host memory).  Replaces the mul / add steps of chi_op and the rescaling of
+ *                 __update_operators (solver.py:514-528).
+ *   mmx_axpby:    out = a x + b y (nwords complex words).
+ */
+int mmx_curl_ft(mmx_plan* plan, const void* F, void* out, void* stream);
+int mmx_green_ft(mmx_plan* plan, void* F, double alpha_re, double alpha_im, void* stream);
+int mmx_chi_mix(const void* x, const void* d, const void* chi_ee, const void* chi_eh, const void* chi_he,
+                const void* chi_hh, const double* coef, void* u, void* w, int64_t nvox, int precision, void* stream);
+int mmx_axpby(void* out, const void* x, const void* y, double a_re, double a_im, double b_re, double b_im,
+              int64_t nwords, int precision, void* stream);
+
+/*
+ * The alpha objective of the preconditioner for a scalar permittivity/*
  * The alpha objective of the preconditioner for a scalar permittivity (replaces the full-grid host evaluation in
  * Solution.__prepare_preconditioner, solver.py:392-401): out_dev[0..1] = min, max over the nvox voxels of
  * (ab^2 - 2 round(x ab)) + p, where xp holds the pairs (x, p) = (Re eps, Re(conj(eps) eps)) in FP64 on the device.

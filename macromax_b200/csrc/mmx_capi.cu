@@ -14,6 +14,7 @@
 #include "mmx_reg.cuh"
 #include "mmx_plane.cuh"
 #include "mmx_epro.cuh"
+#include "mmx_magnetic.cuh"
 
 #define MMX_ABI_VERSION 1
 
@@ -1147,6 +1148,93 @@ extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int m
   k_mat3_extremes<<<blocks, 256, 0, s>>>((const double2*)M, nvox, mode, ab, p->partials);
   MMX_CUDA(cudaGetLastError());
   k_minmax_final<<<1, 256, 0, s>>>(p->partials, blocks, out_dev);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+namespace {
+KGrid kgrid_of(const mmx_plan* p) {
+  KGrid g;
+  g.ndim = p->ndim;
+  for (int i = 0; i < 3; ++i) g.dims[i] = (int)p->shape[i];
+  g.N = p->N;
+  return g;
+}
+template <class R> const R* kv_of(const mmx_plan* p, int axis) {
+  return axis < p->ndim ? (const R*)p->kv_dev + p->kv_off[axis] : nullptr;
+}
+}  // namespace
+
+extern "C" int mmx_curl_ft(mmx_plan* p, const void* F, void* out, void* stream) {
+  if (!p || !F || !out) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
+  if (F == out) return fail(MMX_ERR_ARG, "mmx_curl_ft cannot run in place");
+  cudaStream_t s = (cudaStream_t)stream;
+  const KGrid g = kgrid_of(p);
+  const int blocks = grid_blocks(p->N, 256);
+  if (p->prec == MMX_C128)
+    k_curl_ft<double><<<blocks, 256, 0, s>>>((const double2*)F, (double2*)out, g, kv_of<double>(p, 0),
+                                             kv_of<double>(p, 1), kv_of<double>(p, 2));
+  else
+    k_curl_ft<float><<<blocks, 256, 0, s>>>((const float2*)F, (float2*)out, g, kv_of<float>(p, 0),
+                                            kv_of<float>(p, 1), kv_of<float>(p, 2));
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+extern "C" int mmx_green_ft(mmx_plan* p, void* F, double alpha_re, double alpha_im, void* stream) {
+  if (!p || !F) return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
+  if (!(alpha_im > 0.0)) return fail(MMX_ERR_ARG, "alpha must have a positive imaginary part");
+  cudaStream_t s = (cudaStream_t)stream;
+  const KGrid g = kgrid_of(p);
+  const int blocks = grid_blocks(p->N, 256);
+  if (p->prec == MMX_C128)
+    k_green_ft<double><<<blocks, 256, 0, s>>>((double2*)F, g, kv_of<double>(p, 0), kv_of<double>(p, 1),
+                                              kv_of<double>(p, 2), alpha_re, alpha_im);
+  else
+    k_green_ft<float><<<blocks, 256, 0, s>>>((float2*)F, g, kv_of<float>(p, 0), kv_of<float>(p, 1),
+                                             kv_of<float>(p, 2), (float)alpha_re, (float)alpha_im);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+extern "C" int mmx_chi_mix(const void* x, const void* d, const void* chi_ee, const void* chi_eh, const void* chi_he,
+                           const void* chi_hh, const double* coef, void* u, void* w, int64_t nvox, int precision,
+                           void* stream) {
+  if (!x || !d || !chi_ee || !chi_eh || !chi_he || !chi_hh || !coef || !u || !w)
+    return fail(MMX_ERR_ARG, "NULL buffer");
+  if (nvox < 1) return fail(MMX_ERR_ARG, "nvox must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = grid_blocks(nvox, 256);
+  if (precision == MMX_C128) {
+    auto c = [&](int i) { return make_double2(coef[2 * i], coef[2 * i + 1]); };
+    k_chi_mix<double><<<blocks, 256, 0, s>>>((const double2*)x, (const double2*)d, (const double2*)chi_ee,
+                                             (const double2*)chi_eh, (const double2*)chi_he, (const double2*)chi_hh,
+                                             c(0), c(1), c(2), c(3), c(4), (double2*)u, (double2*)w, nvox);
+  } else {
+    auto c = [&](int i) { return make_float2((float)coef[2 * i], (float)coef[2 * i + 1]); };
+    k_chi_mix<float><<<blocks, 256, 0, s>>>((const float2*)x, (const float2*)d, (const float2*)chi_ee,
+                                            (const float2*)chi_eh, (const float2*)chi_he, (const float2*)chi_hh,
+                                            c(0), c(1), c(2), c(3), c(4), (float2*)u, (float2*)w, nvox);
+  }
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+extern "C" int mmx_axpby(void* out, const void* x, const void* y, double a_re, double a_im, double b_re, double b_im,
+                         int64_t nwords, int precision, void* stream) {
+  if (!out || !x || !y) return fail(MMX_ERR_ARG, "NULL buffer");
+  if (nwords < 1) return fail(MMX_ERR_ARG, "nwords must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = grid_blocks(nwords, 256);
+  if (precision == MMX_C128)
+    k_axpby<double><<<blocks, 256, 0, s>>>((double2*)out, (const double2*)x, (const double2*)y,
+                                           make_double2(a_re, a_im), make_double2(b_re, b_im), nwords);
+  else
+    k_axpby<float><<<blocks, 256, 0, s>>>((float2*)out, (const float2*)x, (const float2*)y,
+                                          make_float2((float)a_re, (float)a_im), make_float2((float)b_re, (float)b_im),
+                                          nwords);
   MMX_CUDA(cudaGetLastError());
   return MMX_OK;
 }

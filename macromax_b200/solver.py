@@ -44,6 +44,23 @@ def solve(grid, vectorial=None, wavenumber=1.0, angular_frequency=None, vacuum_w
 
 
 class Solution:
+    def __new__(cls, grid, vectorial=None, wavenumber=1.0, angular_frequency=None, vacuum_wavelength=None,
+                current_density=None, source_distribution=None, epsilon=None, xi=0.0, zeta=0.0, mu=1.0,
+                refractive_index=None, bound=None, initial_field=0.0, dtype=None, device=None):
+        """Magnetic and bi-(an)isotropic media take the reference's magnetic code path: a MagneticSolution, with
+        the same constructor arguments and properties."""
+        from .magnetic import MagneticSolution, needs_magnetic_solver
+        g = grid
+        if not isinstance(g, Grid):
+            g = Grid.from_ranges(*([g] if np.isscalar(g[0]) else g))
+        if needs_magnetic_solver(g, epsilon, xi, zeta, mu, refractive_index, bound):
+            return MagneticSolution(g, vectorial=vectorial, wavenumber=wavenumber,
+                                    angular_frequency=angular_frequency, vacuum_wavelength=vacuum_wavelength,
+                                    current_density=current_density, source_distribution=source_distribution,
+                                    epsilon=epsilon, xi=xi, zeta=zeta, mu=mu, refractive_index=refractive_index,
+                                    bound=bound, initial_field=initial_field, dtype=dtype, device=device)
+        return super().__new__(cls)
+
     def __init__(self, grid, vectorial=None, wavenumber=1.0, angular_frequency=None, vacuum_wavelength=None,
                  current_density=None, source_distribution=None, epsilon=None, xi=0.0, zeta=0.0, mu=1.0,
                  refractive_index=None, bound=None, initial_field=0.0, dtype=None, device=None):

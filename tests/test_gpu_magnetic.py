@@ -1,0 +1,87 @@
+"""
+Magnetic and bi-(an)isotropic media (macromax_b200/magnetic.py: the reference's magnetic preconditioner and chi_op
+with spectral curls, composed of device kernels) against the reference: its iterates on a negative-index plate and a
+chiral sphere (tests/golden/magnetic2d_48_c128.npz, chiral3d_16_c128.npz) and the known answer of the reference test
+suite's magnetic solve (tests/test_solution.py:360-411).
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm((np.asarray(a) - np.asarray(b)).ravel()) / np.linalg.norm(np.asarray(b).ravel()))
+
+
+def _solution(z, dtype):
+    from macromax_b200 import Bound, Grid, Solution
+    from macromax_b200.magnetic import MagneticSolution
+    grid = Grid(shape=tuple(int(s) for s in z['shape']), step=float(z['step']))
+    sol = Solution(grid, vacuum_wavelength=float(z['wavelength']), epsilon=z['epsilon'], xi=z['xi'], zeta=z['zeta'],
+                   mu=z['mu'], source_distribution=z['source'], bound=Bound(grid, thickness=float(z['bound_thickness'])),
+                   dtype=dtype)
+    assert isinstance(sol, MagneticSolution) and sol.magnetic
+    return sol
+
+
+@pytest.mark.parametrize('name', ['magnetic2d_48_c128', 'chiral3d_16_c128'])
+def test_magnetic_iterates_match_reference(name):
+    z = load_golden(name)
+    sol = _solution(z, np.complex128)
+    assert abs(sol.alpha - complex(z['alpha0'])) <= 1e-12 * abs(complex(z['alpha0']))
+    assert abs(sol.beta - float(z['beta'])) <= 1e-12 * abs(float(z['beta']))
+    record = set(int(r) for r in z['record'])
+    for s in sol:
+        if s.iteration in record:
+            assert rel(s.E, z[f'E{s.iteration}']) < 1e-10, s.iteration
+        if s.iteration >= max(record):
+            break
+    assert abs(sol.alpha - complex(z['alpha_final'])) <= 1e-12 * abs(complex(z['alpha_final']))
+
+
+def test_magnetic_complex64():
+    z = load_golden('chiral3d_16_c128')
+    sol = _solution(z, np.complex64)
+    for s in sol:
+        if s.iteration == 5:
+            assert rel(s.E, z['E5']) < 1e-4
+            break
+
+
+def test_reference_negative_index_plate_known_answer():
+    """The reference's magnetic solve: a -1.5 index plate, 128^2 grid, complex64, to residue 1e-3 in at most 1000
+    iterations, with the field norms in front of and behind the plate that its test asserts to 5 decimals."""
+    from macromax_b200 import Grid, LinearBound, solve
+    wavelength = 500e-9
+    boundary_thickness = 2e-6
+    beam_diameter = 5e-6
+    plate_thickness = 5e-6
+    k0 = 2 * np.pi / wavelength
+    grid = Grid(shape=(128, 128), step=wavelength / 4)
+    angle = 30 * np.pi / 180
+
+    def rot_z(a):
+        return np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1]])
+
+    incident_k = rot_z(angle) * k0 @ np.array([1, 0, 0])
+    polarisation = (rot_z(angle) @ np.array([0, 1, 1j]) / np.sqrt(2))[:, np.newaxis, np.newaxis]
+    current = np.exp(1j * (incident_k[0] * grid[0] + incident_k[1] * grid[1]))
+    source_pixel = grid.shape[0] - int(boundary_thickness / grid.step[0])
+    current[:source_pixel, :] = 0
+    current[source_pixel + 1:, :] = 0
+    current = current * np.exp(-0.5 * ((grid[1] - grid[1].ravel()[grid.shape[0] // 3]) / (beam_diameter / 2)) ** 2)
+    current = current[np.newaxis, ...] * polarisation
+    n = 1 + (-1.5 - 1) * np.ones(grid[1].shape) * (np.abs(grid[0]) < plate_thickness / 2)
+    bound = LinearBound(grid, thickness=boundary_thickness, max_extinction_coefficient=0.50)
+    sol = solve(grid, vacuum_wavelength=wavelength, current_density=current, refractive_index=n, bound=bound,
+                callback=lambda s: s.iteration < 1e4 and s.residue > 1e-3, dtype=np.complex64)
+    assert sol.residue < 1e-3 and sol.iteration <= 1000
+    E = sol.E
+    front = E[:, source_pixel + 1:source_pixel + 8, :]
+    back = E[:, -source_pixel - 8:-source_pixel - 1, :]
+    assert abs(np.linalg.norm(back.ravel()) - 0.0001864) < 1.5e-5  # numpy decimal=5, as in the reference test
+    assert abs(np.linalg.norm(front.ravel()) - 0.0002582) < 1.5e-5
+    assert E.dtype == np.complex64
