@@ -37,8 +37,6 @@ extern "C" {
 #define MMX_STATUS_OK 0
 #define MMX_STATUS_ZERODIV 1 /* update norm 0 after a previous norm of 0: the reference raises ZeroDivisionError */
 #define MMX_STATUS_TIMEOUT 2 /* a bounded wait for an asynchronous shared-memory copy gave up (results kept valid) */
-#define MMX_STATUS_FLOW_TIMEOUT 4 /* a bounded wait of the dataflow schedule for a predecessor tile gave up (results
-                                     of this right-hand side invalid) */
 
 /*
  * Per right-hand-side iteration state, one entry per batch member, in DEVICE memory.  Mirrors the private state of
@@ -172,8 +170,6 @@ int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int 
 #define MMX_VARIANT_PERSISTENT 4u     /* persistent double-buffered prologue/epilogue passes */
 #define MMX_VARIANT_PLANE 8u          /* 3D, 128 x 128 planes, isotropic chi: the two inner axes in one pass */
 #define MMX_VARIANT_FUSED_EPILOGUE 16u /* isotropic chi: epilogue fused with the next prologue (speculative) */
-#define MMX_VARIANT_DATAFLOW 32u      /* 3D, isotropic chi: the axis-0, inverse axis-1 and epilogue passes wait per
-                                         chunk / plane for the tiles they read instead of for the whole previous pass */
 
 /* Select the kernel variant of a plan (rebuilds its pass list, drops its captured graphs).  No reference
  * counterpart: the reference has one implementation per backend. */

@@ -24,13 +24,11 @@ MMX_CHI_MAT3 = 9
 MMX_STATUS_OK = 0
 MMX_STATUS_ZERODIV = 1
 MMX_STATUS_TIMEOUT = 2
-MMX_STATUS_FLOW_TIMEOUT = 4
 MMX_VARIANT_GENERIC = 1
 MMX_VARIANT_SHARED_STAGED = 2
 MMX_VARIANT_PERSISTENT = 4
 MMX_VARIANT_PLANE = 8
 MMX_VARIANT_FUSED_EPILOGUE = 16
-MMX_VARIANT_DATAFLOW = 32
 
 # numpy mirror of struct mmx_rhs_state (include/macromax_b200.h)
 STATE_DTYPE = np.dtype([
@@ -61,13 +59,6 @@ def device_ptr(t) -> ctypes.c_void_p:
     if not t.is_contiguous():
         raise ValueError(f'the C ABI needs contiguous tensors (shape {tuple(t.shape)}, strides {t.stride()})')
     return ctypes.c_void_p(t.data_ptr())
-
-
-def check_flow_status(st) -> None:
-    """Raise if a bounded wait of the dataflow schedule gave up for any right-hand side (its results are invalid)."""
-    import numpy as np
-    if np.any(np.asarray(st['status']) & MMX_STATUS_FLOW_TIMEOUT):
-        raise RuntimeError('a bounded wait between the passes of the dataflow schedule gave up; results are invalid')
 
 
 def load(path: str | None = None):

@@ -109,7 +109,6 @@ class BatchSolution:
 
     def solve(self, rtol: float = 1e-6, maxiter=inf) -> 'BatchSolution':
         st = self.engine.run(float(rtol), float(maxiter))
-        nat.check_flow_status(st)
         if np.any(st['status'] == nat.MMX_STATUS_ZERODIV):
             raise ZeroDivisionError('float division by zero (update norm after a zero update norm)')
         self._state = st

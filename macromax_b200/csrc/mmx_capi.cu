@@ -118,8 +118,6 @@ struct mmx_plan {
   std::vector<PassCfg> plane_passes;  // the 3-pass schedule used when `plane` is set and chi is isotropic
   bool epro = false;           // fuse each epilogue with the next iteration's prologue (isotropic chi)
   std::vector<PassCfg> epro_passes;   // [middle passes..., EPI+PRO, repair]; the first PRO runs once per call
-  bool dataflow = false;       // per-chunk / per-plane tile counters instead of whole-pass waits (3D)
-  unsigned int* flow = nullptr;   // [batch][2 n2/16 + n0] tile counters (zero between iterations)
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
   size_t l2_window = 0;
@@ -658,18 +656,6 @@ std::vector<PassCfg> build_plane_passes(const mmx_plan* p) {
   return v;
 }
 
-// The dataflow schedule needs the 5-pass register-staged 3D schedule: contiguous prologue/epilogue passes whose
-// tiles lie inside one i0 plane, and strided passes on axes 1, 0, 1 with 16-pencil tiles (n2 a multiple of 16).
-bool flow_eligible(const mmx_plan* p) {
-  if (p->ndim != 3 || p->prec != MMX_C64 || p->shape[2] % kRegP != 0) return false;
-  const std::vector<PassCfg>& v = p->iter_passes;
-  if (v.size() != 5 || !v[0].regc || v[0].pipe || !v[4].regc || v[4].pipe) return false;
-  if (!v[1].reg || v[1].axis != 1 || !v[2].reg || v[2].axis != 0 || !v[3].reg || v[3].axis != 1) return false;
-  if (v[4].rc_tiles <= 0 || (p->shape[0] * p->shape[1]) % v[4].rc_tiles != 0) return false;
-  const int64_t pc = p->shape[0] * p->shape[1] / v[4].rc_tiles;  // rows per epilogue tile
-  return p->shape[1] % pc == 0;
-}
-
 template <class R> IterArgs<R> base_args(mmx_plan* p) {
   IterArgs<R> a;
   memset(&a, 0, sizeof(a));
@@ -701,8 +687,6 @@ int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kin
                      !p->plane_passes.empty();
   const bool epro = std::is_same<R, float>::value && !plane && p->epro && chi_kind == MMX_CHI_SCALAR &&
                     !p->epro_passes.empty();
-  if (std::is_same<R, float>::value && !plane && p->dataflow && p->flow && chi_kind == MMX_CHI_SCALAR)
-    a.flow = p->flow;
   if (epro) {
     // first prologue of the chunk, then per iteration the middle passes, the fused epilogue + next prologue and
     // the repair pass
@@ -902,7 +886,6 @@ int mmx_plan_destroy(mmx_plan* p) {
   if (p->work) cudaFree(p->work);
   if (p->partials) cudaFree(p->partials);
   if (p->done) cudaFree(p->done);
-  if (p->flow) cudaFree(p->flow);
   if (p->l2_persist) {  // hand the persisting set-aside back
     cudaCtxResetPersistingL2Cache();
     cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, p->l2_prev_limit);
@@ -1130,7 +1113,7 @@ extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const 
 
 extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
   if (!p) return fail(MMX_ERR_ARG, "NULL plan");
-  if (flags & ~63u) return fail(MMX_ERR_ARG, "unknown variant flags");
+  if (flags & ~31u) return fail(MMX_ERR_ARG, "unknown variant flags");
   drop_graphs_of(p);  // captured graphs hold the previous kernels
   p->force_generic = (flags & MMX_VARIANT_GENERIC) != 0;
   p->no_reg = (flags & MMX_VARIANT_SHARED_STAGED) != 0;
@@ -1141,16 +1124,6 @@ extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
   p->defect_passes = build_passes(p, true);
   p->plane_passes = build_plane_passes(p);
   p->epro_passes = build_epro_passes(p);
-  p->dataflow = (flags & MMX_VARIANT_DATAFLOW) != 0 && flow_eligible(p);
-  if (p->dataflow && !p->flow) {
-    const size_t bytes = sizeof(unsigned int) * (size_t)p->batch * (size_t)(2 * (p->shape[2] / kRegP) + p->shape[0]);
-    cudaError_t e = cudaMalloc(&p->flow, bytes);
-    if (e == cudaSuccess) e = cudaMemset(p->flow, 0, bytes);
-    if (e != cudaSuccess) {
-      p->dataflow = false;
-      return cuda_fail(e, "cudaMalloc(flow counters)");
-    }
-  }
   for (const auto* list : {&p->iter_passes, &p->plane_passes, &p->epro_passes})
     for (auto& pc : *list)
       if (2 * (int64_t)p->batch * pc.tiles > p->partials_len) return fail(MMX_ERR_ARG, "internal: partials too small");
@@ -1161,7 +1134,7 @@ extern "C" unsigned mmx_plan_get_variant(const mmx_plan* p) {
   if (!p) return 0u;
   return (p->force_generic ? MMX_VARIANT_GENERIC : 0u) | (p->no_reg ? MMX_VARIANT_SHARED_STAGED : 0u) |
          (p->pipe ? MMX_VARIANT_PERSISTENT : 0u) | (p->plane ? MMX_VARIANT_PLANE : 0u) |
-         (p->epro ? MMX_VARIANT_FUSED_EPILOGUE : 0u) | (p->dataflow ? MMX_VARIANT_DATAFLOW : 0u);
+         (p->epro ? MMX_VARIANT_FUSED_EPILOGUE : 0u);
 }
 
 extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,

@@ -142,17 +142,9 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, 
 #pragma unroll
     for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(a.src + ((int64_t)b * C + cc2) * N3 + row0, chunk);
   }
-  if (a.flow != nullptr) {
-    // dataflow schedule: wait for the inverse axis-1 tiles of this tile's i0 plane only
-    pdl_trigger();
-    if (!flow_active(st)) return;
-    const int i0 = (int)(((int64_t)blockIdx.x * PC) / a.dims[1]);
-    flow_wait(a.flow + (int64_t)b * flow_stride(a) + 2 * (a.dims[2] / 16) + i0, (unsigned)(a.dims[2] / 16), st);
-  } else {
-    pdl_wait();
-    pdl_trigger();
-    if (!st->active) return;
-  }
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
   const ChiCoef<float> cc = chi_coef<float>(st);
   const int tid = threadIdx.x;
   const int ii = tid % TPP;

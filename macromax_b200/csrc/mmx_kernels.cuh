@@ -11,8 +11,6 @@
 // d = chi (T - E), E_new = E + d written to the other field buffer, with per-CTA partial sums of |d|^2 and |E_new|^2
 // reduced in a fixed order by the last tile of each right-hand side, which then takes the accept/reject decision.
 #pragma once
-#include <type_traits>
-
 #include "../../include/macromax_b200.h"
 #include "mmx_fft.cuh"
 
@@ -47,7 +45,6 @@ template <class R> struct IterArgs {
   float2* aux;           // defect output [B][C][N] complex64
   size_t l2_window;      // bytes of T kept L2-resident (0: off); host-side launch attribute only
   int nrhs;              // number of right-hand sides (persistent passes)
-  unsigned int* flow;    // tile-completion counters of the dataflow schedule [B][2 nc + n0] (nullptr: off)
 };
 
 // Programmatic dependent launch.  The pass kernels are launched so that the next pass's CTAs may become resident
@@ -57,62 +54,6 @@ template <class R> struct IterArgs {
 // Both are no-ops for a kernel launched without the attribute.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-// Dataflow between the passes of the 3D schedule (3D grids, register-staged passes).  Instead of waiting for the
-// whole previous grid (pdl_wait), a tile of the axis-0 pass, of the inverse axis-1 pass and of the epilogue pass
-// waits only for the tiles of the previous pass that wrote its inputs, counted per chunk of 16 consecutive i2
-// (nc = n2 / 16 chunks) or per i0 plane:
-//   forward axis-1 tiles (i0, chunk)  -> cnt[chunk]            (n0 per chunk)
-//   axis-0 tiles (i1, chunk)           -> cnt[nc + chunk]       (n1 per chunk)
-//   inverse axis-1 tiles (i0, chunk)   -> cnt[2 nc + i0]        (nc per plane)
-// The strided passes take their tiles chunk-major, so the next pass finds whole chunks finished while the
-// previous one is still running, and its CTAs fill the SMs that the previous pass's last wave leaves idle.
-// A producer publishes a tile after all its stores (barrier, fence, atomic add); a consumer's thread 0 polls with
-// acquire loads and the block passes a barrier before reading.  A pass's CTAs start only once every CTA of the
-// previous pass has started (programmatic launch), so every tile waited on is resident or done: the waits end.
-// They are bounded all the same: after kFlowMaxPolls polls the wait gives up and marks the right-hand side
-// MMX_STATUS_FLOW_TIMEOUT (the results of that solve are then invalid and the host raises).  The last tile of the
-// epilogue pass of each right-hand side, which takes the accept/reject decision, resets its counters: no tile of
-// the iteration reads them any more, and the next writes come after the next pdl_wait.
-constexpr int kFlowMaxPolls = 1 << 21;
-
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ int ld_relaxed_s32(const int* p) {
-  int v;
-  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// `active` of a right-hand side read past the L1 cache (the decision that wrote it finished before this pass began)
-__device__ __forceinline__ bool flow_active(const mmx_rhs_state* st) { return ld_relaxed_s32(&st->active) != 0; }
-
-__device__ __forceinline__ int flow_stride(const IterArgs<float>& a) { return 2 * (a.dims[2] / 16) + a.dims[0]; }
-
-__device__ __forceinline__ void flow_wait(const unsigned* cnt, unsigned target, const mmx_rhs_state* st) {
-  if (threadIdx.x == 0) {
-    int* status = const_cast<int*>(&st->status);
-    for (int polls = 0; ld_acquire_u32(cnt) < target; ++polls) {
-      if (polls >= kFlowMaxPolls || ((polls & 1023) == 1023 && (ld_relaxed_s32(status) & MMX_STATUS_FLOW_TIMEOUT))) {
-        atomicOr(status, MMX_STATUS_FLOW_TIMEOUT);
-        break;
-      }
-      __nanosleep(64);
-    }
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void flow_signal(unsigned* cnt) {
-  __syncthreads();  // every store of the tile has been issued
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(cnt, 1u);
-  }
-}
 
 // |z|^2 accumulated in FP64 (the squares of complex64 words are exact in double)
 __device__ __forceinline__ double norm2d(float2 z) { return (double)z.x * z.x + (double)z.y * z.y; }
@@ -460,12 +401,6 @@ __device__ __forceinline__ void finish_pass_norms(const IterArgs<R>& a, int b, d
     __threadfence();
     decide_rhs(const_cast<mmx_rhs_state*>(a.st) + b, a.partials + (int64_t)b * gridDim.x * 2, gridDim.x);
     if (threadIdx.x == 0) a.done[b] = 0u;
-    if constexpr (std::is_same<R, float>::value) {
-      if (a.flow) {
-        const int fs = flow_stride(a);
-        for (int t = threadIdx.x; t < fs; t += blockDim.x) a.flow[(int64_t)b * fs + t] = 0u;
-      }
-    }
   }
 }
 

@@ -250,14 +250,21 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 }
 
 // OPS: OP_FWD (forward pass), OP_INV (inverse pass) or OP_FWD | OP_G | OP_INV (axis-0 pass with the Green multiply)
-// One tile (16 consecutive pencils from pencil p0) of a strided pass.
 template <int C, int OPS, int N>
-__device__ __forceinline__ void reg_pass_tile(const IterArgs<float>& a, int b, const mmx_rhs_state* st,
-                                              int64_t p0, float2* sm, float2* smtw) {
+__global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArgs<float> a) {
   constexpr int P = kRegP;
   constexpr int THREADS = RegThreads<C, N>::value;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * N * P;
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
   const int tid = threadIdx.x;
   const int64_t inner = a.inner;
+  const int64_t p0 = (int64_t)blockIdx.x * P;
   const int64_t o = p0 / inner;
   const int64_t in0 = p0 - o * inner;
   float2* tile = a.T + (int64_t)b * C * a.N + o * (int64_t)N * inner + in0;
@@ -379,51 +386,6 @@ __device__ __forceinline__ void reg_pass_tile(const IterArgs<float>& a, int b, c
     }
     __syncthreads();
     rfft<+1, N, C, false, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
-  }
-}
-
-template <int C, int OPS, int N>
-__global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArgs<float> a) {
-  constexpr int P = kRegP;
-  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
-  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
-  float2* smtw = sm + C * N * P;
-  const int b = blockIdx.y;
-  const mmx_rhs_state* st = a.st + b;
-  if (a.flow == nullptr) {
-    pdl_wait();
-    pdl_trigger();
-    if (!st->active) return;
-    reg_pass_tile<C, OPS, N>(a, b, st, (int64_t)blockIdx.x * P, sm, smtw);
-    return;
-  }
-  // dataflow schedule (3D): tiles chunk-major, i.e. tile = chunk * K + j with pencil p0 = j n2 + 16 chunk, where
-  // j = i0 (axis-1 passes, K = n0) or i1 (axis-0 pass, K = n1)
-  const int n2 = a.dims[2];
-  const int nc = n2 / P;
-  const int64_t K = (int64_t)gridDim.x / nc;
-  const int64_t chunk = (int64_t)blockIdx.x / K;
-  const int64_t j = (int64_t)blockIdx.x - chunk * K;
-  const int64_t p0 = j * n2 + chunk * P;
-  unsigned int* cnt = a.flow + (int64_t)b * flow_stride(a);
-  if constexpr (OPS == OP_FWD) {
-    pdl_wait();  // the previous iteration's epilogue (and its decision) as a whole
-    pdl_trigger();
-    if (!st->active) return;
-    reg_pass_tile<C, OPS, N>(a, b, st, p0, sm, smtw);
-    flow_signal(cnt + chunk);
-  } else if constexpr (OPS == OP_INV) {
-    pdl_trigger();
-    if (!flow_active(st)) return;
-    flow_wait(cnt + nc + chunk, (unsigned)a.dims[1], st);
-    reg_pass_tile<C, OPS, N>(a, b, st, p0, sm, smtw);
-    flow_signal(cnt + 2 * nc + j);
-  } else {
-    pdl_trigger();
-    if (!flow_active(st)) return;
-    flow_wait(cnt + chunk, (unsigned)a.dims[0], st);
-    reg_pass_tile<C, OPS, N>(a, b, st, p0, sm, smtw);
-    flow_signal(cnt + nc + chunk);
   }
 }
 
@@ -614,17 +576,9 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
       for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(a.src + ((int64_t)b * C + cc2) * a.N + row0, chunk);
     }
   }
-  if ((OPS & OP_EPI) != 0 && a.flow != nullptr) {
-    // dataflow schedule: wait for the inverse axis-1 tiles of this tile's i0 plane only
-    pdl_trigger();
-    if (!flow_active(st)) return;
-    const int i0 = (int)(((int64_t)blockIdx.x * PC) / a.dims[1]);
-    flow_wait(a.flow + (int64_t)b * flow_stride(a) + 2 * (a.dims[2] / 16) + i0, (unsigned)(a.dims[2] / 16), st);
-  } else {
-    pdl_wait();
-    pdl_trigger();
-    if (!st->active) return;
-  }
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
   const ChiCoef<float> cc = chi_coef<float>(st);
   const int tid = threadIdx.x;
   const int ii = tid % TPP;

@@ -310,7 +310,6 @@ class Solution:
         return int(self._state['rejections'])
 
     def _check_status(self, st):
-        nat.check_flow_status(st)
         if int(st['status']) == nat.MMX_STATUS_ZERODIV:
             raise ZeroDivisionError('float division by zero (update norm after a zero update norm)')
 
