@@ -280,6 +280,7 @@ def run_secondary(args):
       - 2D scalar 256^2 disks in complex128 to 1e-6 or 500 iterations, set-up included;
       - 3D anisotropic 192^3 Voronoi grains, complex64 inner iterations with FP64 defect correction, to 1e-8;
       - a magnetic medium (the reference test suite's negative-index plate, 128^2) to residue 1e-3;
+      - the full scattering matrix of a 512 x 256 slab (254 columns in batched solves);
       - batched mixed precision (2D scalar slab, 512^2 grid, 256 plane-wave sources) to residue 1e-8, against the
         plain complex64 per-source loop (one Solution per source, to 1e-5: single precision cannot reach 1e-8),
         measured on 4 sources and scaled to 256;
@@ -378,6 +379,28 @@ def run_secondary(args):
     out['magnetic_negative_index_plate_128'] = {'time_to_1e-3_s (set-up included)': b - a,
                                                 'iterations': int(sol.iteration), 'residue': float(sol.residue)}
     sol.close()
+    # scattering matrix: every column of a 512 x 256 grid holding a 128-px layer of the correlated-disorder slab
+    # across axis 0, periodic across, absorbing 32-px layers at both ends of axis 0
+    from macromax_b200.matrix import ScatteringMatrix
+    wl = workloads.correlated_slab_2d(n=512)
+    start = (512 - 128) // 2
+    eps = np.ones((512, 256), dtype=np.complex128)
+    eps[start:start + 128, :] = wl['epsilon'][16:272, start:start + 128].T
+    grid = Grid(shape=(512, 256), step=wl['step'])
+    thickness = np.zeros((2, 1))
+    thickness[0, 0] = 32 * wl['step']
+    sm = ScatteringMatrix(grid, vectorial=False, vacuum_wavelength=wl['wavelength'], epsilon=eps,
+                          bound=LinearBound(grid, thickness=thickness, max_extinction_coefficient=0.25),
+                          dtype=np.complex64)
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    _ = sm._solution  # set-up (preconditioner) of the shared material
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    S = np.asarray(sm)
+    c = time.perf_counter()
+    out['scattering_matrix_slab2d_512x256'] = {'columns': int(S.shape[1]), 'setup_s': b - a, 'columns_s': c - b}
+    del S, sm
     wl = workloads.design_3d(n=128, nb_sources=32)
     grid = Grid(shape=wl['shape'], step=wl['step'])
     k0 = 2 * np.pi / wl['wavelength']

@@ -211,7 +211,6 @@ int mmx_axpby(void* out, const void* x, const void* y, double a_re, double a_im,
               int64_t nwords, int precision, void* stream);
 
 /*
- * The alpha objective of the preconditioner for a scalar permittivity/*
  * The alpha objective of the preconditioner for a scalar permittivity (replaces the full-grid host evaluation in
  * Solution.__prepare_preconditioner, solver.py:392-401): out_dev[0..1] = min, max over the nvox voxels of
  * (ab^2 - 2 round(x ab)) + p, where xp holds the pairs (x, p) = (Re eps, Re(conj(eps) eps)) in FP64 on the device.
@@ -222,7 +221,15 @@ int mmx_axpby(void* out, const void* x, const void* y, double a_re, double a_im,
 int mmx_scalar_sigma(mmx_plan* plan, const void* xp, int64_t nvox, double ab, double* out_dev, void* stream);
 
 /*
- * mmx_fftn without a plan and without any device allocation:/*
+ * The susceptibility at the preconditioner's alpha from a permittivity already on the device (replaces the host
+ * array expression of Solution.__prepare_preconditioner, solver.py:480-484, chi = eps i / (alpha_i beta) - i alpha /
+ * alpha_i I):  chi[r][v] = s eps[r][v] - (r on the diagonal ? d : 0) for the m = 1 or 9 row-major entries of a
+ * complex128 matrix field eps [m][nvox]; chi is written in `precision` (complex64 or complex128), s and d in FP64.
+ */
+int mmx_chi_from_eps(const void* eps, int m, int64_t nvox, double s_re, double s_im, double d_re, double d_im,
+                     void* chi, int precision, void* stream);
+
+/*
  * mmx_fftn without a plan and without any device allocation: the same transform as mmx_fftn (forward unscaled,
  * inverse scaled by 1/N) over the `ndim` grid axes `shape` of `nbatch` contiguous fields of the given precision.
  * No counterpart in the reference (which always allocates through its backend).  For callers that must not let a

@@ -44,7 +44,7 @@ EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destro
             'mmx_fftn', 'mmx_norm', 'mmx_iterate', 'mmx_defect', 'mmx_accumulate', 'mmx_adjoint_grad',
             'mmx_pointwise_mul', 'mmx_fftn_noalloc', 'mmx_mat3_extremes', 'mmx_iterate_graph',
             'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant',
-            'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby']
+            'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby', 'mmx_chi_from_eps']
 
 _lib = None
 
@@ -89,6 +89,7 @@ def load(path: str | None = None):
         'mmx_pointwise_mul': (i32, [vp, i32, i32, vp, i32, i32, vp, i64, i32, vp]),
         'mmx_fftn_noalloc': (i32, [i32, ctypes.POINTER(i64), vp, vp, i64, i32, i32, vp]),
         'mmx_scalar_sigma': (i32, [vp, vp, i64, dbl, vp, vp]),
+        'mmx_chi_from_eps': (i32, [vp, i32, i64, dbl, dbl, dbl, dbl, vp, i32, vp]),
         'mmx_curl_ft': (i32, [vp, vp, vp, vp]),
         'mmx_green_ft': (i32, [vp, vp, dbl, dbl, vp]),
         'mmx_chi_mix': (i32, [vp, vp, vp, vp, vp, vp, ctypes.POINTER(dbl), vp, vp, i64, i32, vp]),

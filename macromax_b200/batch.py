@@ -76,10 +76,10 @@ class BatchSolution:
             self.pre, self.bound = prepare_material(grid, epsilon, bound, self.wavenumber, self.dtype, device=device)
         else:
             self.pre, self.bound = preconditioner, bound
-        if self.pre.chi.shape[0] > 1 and self.ncomp != 3:
+        if self.pre.chi_rows > 1 and self.ncomp != 3:
             raise ValueError('an anisotropic permittivity needs vector sources')
         self.engine = IterationEngine(grid.shape, self.ncomp, self.batch, self.dtype, (grid * self.wavenumber).k,
-                                      self.pre.chi, self.pre.alpha, device=device)
+                                      self.pre.chi_for_engine(), self.pre.alpha, device=device)
         self.set_sources(src)
 
     @property

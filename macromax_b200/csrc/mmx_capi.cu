@@ -1252,6 +1252,23 @@ extern "C" int mmx_scalar_sigma(mmx_plan* p, const void* xp, int64_t nvox, doubl
   return MMX_OK;
 }
 
+extern "C" int mmx_chi_from_eps(const void* eps, int m, int64_t nvox, double s_re, double s_im, double d_re,
+                                double d_im, void* chi, int precision, void* stream) {
+  if (!eps || !chi) return fail(MMX_ERR_ARG, "NULL buffer");
+  if (m != 1 && m != 9) return fail(MMX_ERR_ARG, "m must be 1 or 9");
+  if (nvox < 1) return fail(MMX_ERR_ARG, "nvox must be positive");
+  if (precision != MMX_C64 && precision != MMX_C128) return fail(MMX_ERR_ARG, "unknown precision");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int blocks = grid_blocks((int64_t)m * nvox, 256);
+  const double2 sc = make_double2(s_re, s_im), dc = make_double2(d_re, d_im);
+  if (precision == MMX_C64)
+    k_chi_from_eps<float2><<<blocks, 256, 0, s>>>((const double2*)eps, m, nvox, sc, dc, (float2*)chi);
+  else
+    k_chi_from_eps<double2><<<blocks, 256, 0, s>>>((const double2*)eps, m, nvox, sc, dc, (double2*)chi);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Allocation-free N-D FFT.
 //

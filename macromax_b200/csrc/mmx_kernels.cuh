@@ -623,6 +623,27 @@ __global__ void k_mat3_extremes(const double2* __restrict__ M, int64_t N, int mo
 // the real part (ab^2 - 2 round(x ab)) + p with x = Re eps and p = the host's value of Re(conj(eps) eps).  Evaluated
 // here with explicitly rounded FP64 operations (no fused multiply-add), so min / max over the voxels are those of
 // the host expression bit for bit.  xp: [N] pairs (x, p).  Per-block (min, max) partials as k_mat3_extremes.
+// chi = s eps - d I per voxel (m = 1 or 9 row-major entries), from complex128 to the precision of OUT
+template <class OUT>
+__global__ void k_chi_from_eps(const double2* __restrict__ eps, int m, int64_t N, double2 s, double2 d,
+                               OUT* __restrict__ chi) {
+  const int64_t total = (int64_t)m * N;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / N);
+    const double2 e = eps[i];
+    double2 c = make_double2(s.x * e.x - s.y * e.y, s.x * e.y + s.y * e.x);
+    if (m == 1 || r == 0 || r == 4 || r == 8) {
+      c.x -= d.x;
+      c.y -= d.y;
+    }
+    if constexpr (std::is_same<OUT, float2>::value) {
+      chi[i] = make_float2((float)c.x, (float)c.y);
+    } else {
+      chi[i] = c;
+    }
+  }
+}
+
 __global__ void k_scalar_sigma(const double2* __restrict__ xp, int64_t N, double ab, double* part) {
   double vmin = INFINITY, vmax = -INFINITY;
   const double ab2 = __dmul_rn(ab, ab);

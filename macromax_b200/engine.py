@@ -70,8 +70,19 @@ class IterationEngine:
         self.write_state(st)
 
     # -- material ---------------------------------------------------------------------------------------------------
-    def set_chi(self, chi0: np.ndarray, alpha0: complex):
-        """chi0: matrix field [1|3, 1|3, *grid-broadcastable] at alpha0 (expanded to the full grid here)."""
+    def set_chi(self, chi0, alpha0: complex):
+        """chi0: matrix field [1|3, 1|3, *grid-broadcastable] at alpha0 (expanded to the full grid here), or a device
+        tensor [m, N] (m = 1 or 9), used without a host round trip."""
+        if isinstance(chi0, torch.Tensor):
+            m = int(chi0.shape[0])
+            if m not in (1, 9) or chi0.dim() != 2 or int(chi0.shape[1]) != self.N:
+                raise ValueError('a device chi must be [1 or 9, N]')
+            if m == 9 and self.ncomp != 3:
+                raise ValueError('an anisotropic susceptibility needs a vector field')
+            self.chi_kind = nat.MMX_CHI_SCALAR if m == 1 else nat.MMX_CHI_MAT3
+            self.chi = chi0.to(self.device, self.torch_dtype).contiguous()
+            self.alpha0 = complex(alpha0)
+            return
         chi0 = np.asarray(chi0)
         m = chi0.shape[0] * chi0.shape[1]
         if m not in (1, 9):

@@ -249,6 +249,27 @@ class ScatteringMatrix:
             out[:, :, plane] = self._freespace_planes(masked, [plane])[:, :, 0]
         return out
 
+    def _source_plane_fields(self, vectors: np.ndarray) -> np.ndarray:
+        """The nonzero part of _sources: the fields on the back and front source planes, [B, C, 2, *transverse]."""
+        scaled = vectors * self._source_scale()
+        out = []
+        for side in range(2):
+            masked = np.zeros_like(scaled)
+            masked[:, side] = scaled[:, side]
+            out.append(self._freespace_planes(masked, [self._source_planes[side]])[:, :, 0])
+        return np.stack(out, axis=2)
+
+    def _device_sources(self, vectors: np.ndarray) -> torch.Tensor:
+        """_sources built on the device from the two source planes: only [B, C, 2, *transverse] crosses the host link
+        and no dense host array of the batch's size is made."""
+        device = torch.device(self._device if self._device is not None else 'cuda')
+        planes = torch.from_numpy(np.ascontiguousarray(self._source_plane_fields(vectors))).to(device)
+        B, C = planes.shape[:2]
+        src = torch.zeros((B, C, *(int(n) for n in self._grid.shape)), dtype=planes.dtype, device=device)
+        for side in range(2):  # in _sources' order: a shared plane keeps the front side's field
+            src[:, :, self._source_planes[side]] = planes[:, :, side]
+        return src
+
     def srcvec2source(self, input_vector, out: np.ndarray = None) -> np.ndarray:
         """The source field at the front and back source planes for the vector (matrix.py:612-648)."""
         src = self._sources(self._as_modes(input_vector)[None])[0]
@@ -339,11 +360,12 @@ class ScatteringMatrix:
         rtol, maxiter = _DEFAULT_RTOL, _DEFAULT_MAXITER
         for b0 in range(0, B, chunk):
             sl = slice(b0, min(B, b0 + chunk))
-            src = self._sources(vectors[sl])
+            src = self._device_sources(vectors[sl])
             bs = BatchSolution(self._grid, src, None, bound=bound, wavenumber=k0, dtype=self._dtype,
                                device=self._device, preconditioner=pre)
+            del src
             bs.solve(rtol=rtol, maxiter=maxiter)
-            E = bs.E_device.reshape(src.shape[0], nb_pol, *(int(n) for n in self._grid.shape))
+            E = bs.E_device.reshape(bs.batch, nb_pol, *(int(n) for n in self._grid.shape))
             det = torch.stack([E[:, :, p] for p in self._detector_planes], dim=2)
             det = det.cpu().numpy().astype(self._dtype) / (k0 ** 2)
             bs.close()

@@ -56,10 +56,13 @@ class MixedSolution:
         with torch.cuda.device(self.device):
             self.plan64 = nat.Plan(grid.shape, self.ncomp, self.batch, nat.MMX_C128)
             self.plan64.set_kvectors([np.asarray(k, dtype=np.float64).ravel() for k in (grid * self.wavenumber).k])
-            m = pre.chi.shape[0] * pre.chi.shape[1]
-            chi = np.broadcast_to(pre.chi, (pre.chi.shape[0], pre.chi.shape[1], *grid.shape)).reshape(m, N)
-            # C order explicitly: a permittivity built as a strided view reshapes to a strided view too
-            self.chi64 = torch.from_numpy(np.ascontiguousarray(chi, dtype=np.complex128)).to(self.device)
+            if pre.chi_device is not None and int(pre.chi_device.shape[1]) == N:
+                self.chi64 = pre.chi_device.to(self.device, torch.complex128).contiguous()
+            else:
+                m = pre.chi.shape[0] * pre.chi.shape[1]
+                chi = np.broadcast_to(pre.chi, (pre.chi.shape[0], pre.chi.shape[1], *grid.shape)).reshape(m, N)
+                # C order explicitly: a permittivity built as a strided view reshapes to a strided view too
+                self.chi64 = torch.from_numpy(np.ascontiguousarray(chi, dtype=np.complex128)).to(self.device)
             s0 = src.reshape(self.batch, self.ncomp, N) * (1.0j / pre.alpha.imag / pre.beta)
             self.src64 = torch.from_numpy(np.ascontiguousarray(s0, dtype=np.complex128)).to(self.device)
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)

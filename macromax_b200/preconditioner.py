@@ -11,7 +11,6 @@ This runs once per material, not per iteration.
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass
 
 import numpy as np
 import scipy.optimize
@@ -69,13 +68,35 @@ def increase_bias(alpha: complex, thickness: np.ndarray, wavenumber: float, max_
     return complex(alpha.real, offset)
 
 
-@dataclass
 class Preconditioner:
-    alpha: complex
-    beta: float
-    transpose: bool
-    chi: np.ndarray        # [1|3, 1|3, *shape] complex128, i (eps - alpha) / alpha_i (beta = 1)
-    eps_field: np.ndarray  # [1|3, 1|3, *shape] complex128
+    """
+    alpha, beta and the susceptibility chi = eps i / (alpha_i beta) - i alpha / alpha_i I at alpha (solver.py:480-484).
+    chi is held either as a host matrix field [1|3, 1|3, *shape] or, for a 3x3 permittivity whose set-up ran on the
+    device, as a device tensor [m, nvox] complex128 (``chi_device``); ``chi`` copies the latter to the host on first use.
+    """
+
+    def __init__(self, alpha: complex, beta: float, transpose: bool, chi=None, eps_field=None, chi_device=None):
+        self.alpha, self.beta, self.transpose = alpha, beta, transpose
+        self.eps_field = eps_field
+        self._chi = chi
+        self.chi_device = chi_device
+
+    @property
+    def chi_rows(self) -> int:
+        if self.chi_device is not None:
+            return 3 if self.chi_device.shape[0] == 9 else 1
+        return int(self._chi.shape[0])
+
+    @property
+    def chi(self) -> np.ndarray:
+        if self._chi is None:
+            r = self.chi_rows
+            self._chi = self.chi_device.cpu().numpy().reshape(r, r, *self.eps_field.shape[2:])
+        return self._chi
+
+    def chi_for_engine(self):
+        """The device tensor when there is one (no host round trip), else the host matrix field."""
+        return self.chi_device if self.chi_device is not None else self._chi
 
 
 class DeviceSetup:
@@ -116,6 +137,18 @@ class DeviceSetup:
         lo, hi = self._run(1, 0.0)
         thr = math.sqrt(eps_dtype)
         return bool(lo < -thr), bool(hi > thr)
+
+    def chi(self, alpha: complex, beta: float):
+        """chi = eps i / (alpha_i beta) - i alpha / alpha_i I (solver.py:480-484) from the permittivity already on the
+        device (``mmx_chi_from_eps``), as a complex128 device tensor [9, nvox]."""
+        c = self._ctypes
+        s = self._torch.cuda.current_stream().cuda_stream
+        sc = 1.0j / alpha.imag / beta
+        d = alpha * 1.0j / alpha.imag
+        out = self._torch.empty_like(self.M)
+        self._nat.call('mmx_chi_from_eps', c.c_void_p(self.M.data_ptr()), 9, self.nvox, sc.real, sc.imag, d.real,
+                       d.imag, c.c_void_p(out.data_ptr()), self._nat.MMX_C128, c.c_void_p(s) if s else None)
+        return out
 
 
 class ScalarDeviceObjective:
@@ -189,6 +222,9 @@ def prepare(eps_field: np.ndarray, thickness: np.ndarray, wavenumber: float, eps
         alpha = alpha.conjugate()
     alpha = increase_bias(alpha, thickness, wavenumber)
     # solver.py:480-484 (beta == 1 / mu)
+    if dev is not None and dev.nvox == int(np.prod(eps_field.shape[2:])):
+        return Preconditioner(alpha=alpha, beta=beta, transpose=transpose, eps_field=eps_field,
+                              chi_device=dev.chi(alpha, beta))
     chi = eps_field * (1.0j / alpha.imag / beta)
     if _is_scalar_field(chi):
         chi = chi - alpha * 1.0j / alpha.imag

@@ -151,10 +151,10 @@ class Solution:
         alpha = self._pre.alpha
         if self._engine is None:
             self._engine = IterationEngine(self._grid.shape, self._nb_pol, 1, self._dtype, self._k_grid.k,
-                                           self._pre.chi, alpha, device=self._device)
+                                           self._pre.chi_for_engine(), alpha, device=self._device)
             self.E = initial_field
         else:
-            self._engine.rebase_alpha(self._pre.chi, alpha)
+            self._engine.rebase_alpha(self._pre.chi_for_engine(), alpha)
         self.source_distribution = source_distribution
 
     @property

@@ -67,6 +67,24 @@ def test_device_setup_reductions_match_host():
     assert abs(pre.alpha - complex(z['alpha0'])) <= 1e-12 * abs(pre.alpha)
 
 
+def test_device_chi_matches_host_expression():
+    """A 3x3 permittivity's chi is built on the device from the permittivity the set-up already uploaded; it equals
+    the host expression eps i / (alpha_i beta) - i alpha / alpha_i I (solver.py:480-484) to rounding, and the solve
+    that uses it equals the reference's iterates."""
+    from macromax_b200 import preconditioner as pc
+    z = load_golden('voronoi3d_16_c128')
+    eps = np.asarray(z['epsilon'])
+    e = float(np.finfo(np.complex128).eps)
+    thickness = np.broadcast_to(float(z['bound_thickness']), (3, 2))
+    pre = pc.prepare(eps, thickness, 2 * np.pi / float(z['wavelength']), e, device_setup=True)
+    assert pre.chi_device is not None and pre.chi_rows == 3
+    host = eps * (1.0j / pre.alpha.imag / pre.beta) - np.eye(3).reshape(3, 3, 1, 1, 1) * (pre.alpha * 1.0j /
+                                                                                         pre.alpha.imag)
+    dev = pre.chi_device.cpu().numpy().reshape(host.shape)
+    assert rel(dev, host) < 1e-15
+    assert np.array_equal(pre.chi, dev)
+
+
 def test_device_gain_loss_flags_on_lossy_and_gain_media():
     from macromax_b200 import preconditioner as pc
     e = float(np.finfo(np.complex128).eps)
