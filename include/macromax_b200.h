@@ -211,6 +211,27 @@ int mmx_axpby(void* out, const void* x, const void* y, double a_re, double a_im,
               int64_t nwords, int precision, void* stream);
 
 /*
+ * The magnetic iteration on the device: niter iterations of Solution.__iter__ (solver.py:1049-1098) with the
+ * magnetic chi_op (solver.py:531-552), the same composition as the kernels above, but with alpha read from and the
+ * accept / reject (solver.py:1077-1096) and stop rules (solver.py:81-83) taken in the mmx_rhs_state `st`, so that a
+ * chunk of iterations needs no host round trip.  An iteration after which the stop rule fails leaves the state and E
+ * unchanged.  `plan`: 1 component, batch 1, the grid's k-vectors set.  use_graph != 0 replays the chunk from a CUDA
+ * graph captured on the first call with these buffers and niter.  All buffers [3][N] (blocks [9][N]) in the plan's
+ * precision.
+ */
+typedef struct mmx_magnetic_buffers {
+  void* E;            /* the field (times k0^2), updated in place */
+  const void* src;    /* normalised source s'0 at alpha0 */
+  const void* chi_ee; /* the four susceptibility blocks at alpha0, [9][N] each */
+  const void* chi_eh;
+  const void* chi_he;
+  const void* chi_hh;
+  void* work[7];      /* scratch, [3][N] each */
+} mmx_magnetic_buffers;
+int mmx_magnetic_iterate(mmx_plan* plan, const mmx_magnetic_buffers* buffers, mmx_rhs_state* st, int niter,
+                         int use_graph, void* stream);
+
+/*
  * The alpha objective of the preconditioner for a scalar permittivity (replaces the full-grid host evaluation in
  * Solution.__prepare_preconditioner, solver.py:392-401): out_dev[0..1] = min, max over the nvox voxels of
  * (ab^2 - 2 round(x ab)) + p, where xp holds the pairs (x, p) = (Re eps, Re(conj(eps) eps)) in FP64 on the device.

@@ -44,7 +44,8 @@ EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destro
             'mmx_fftn', 'mmx_norm', 'mmx_iterate', 'mmx_defect', 'mmx_accumulate', 'mmx_adjoint_grad',
             'mmx_pointwise_mul', 'mmx_fftn_noalloc', 'mmx_mat3_extremes', 'mmx_iterate_graph',
             'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant',
-            'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby', 'mmx_chi_from_eps']
+            'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby', 'mmx_chi_from_eps',
+            'mmx_magnetic_iterate']
 
 _lib = None
 
@@ -59,6 +60,13 @@ def device_ptr(t) -> ctypes.c_void_p:
     if not t.is_contiguous():
         raise ValueError(f'the C ABI needs contiguous tensors (shape {tuple(t.shape)}, strides {t.stride()})')
     return ctypes.c_void_p(t.data_ptr())
+
+
+class MagneticBuffers(ctypes.Structure):
+    """mmx_magnetic_buffers: the field, source and susceptibility blocks and seven scratch fields (device)."""
+    _fields_ = [('E', ctypes.c_void_p), ('src', ctypes.c_void_p), ('chi_ee', ctypes.c_void_p),
+                ('chi_eh', ctypes.c_void_p), ('chi_he', ctypes.c_void_p), ('chi_hh', ctypes.c_void_p),
+                ('work', ctypes.c_void_p * 7)]
 
 
 def load(path: str | None = None):
@@ -90,6 +98,7 @@ def load(path: str | None = None):
         'mmx_fftn_noalloc': (i32, [i32, ctypes.POINTER(i64), vp, vp, i64, i32, i32, vp]),
         'mmx_scalar_sigma': (i32, [vp, vp, i64, dbl, vp, vp]),
         'mmx_chi_from_eps': (i32, [vp, i32, i64, dbl, dbl, dbl, dbl, vp, i32, vp]),
+        'mmx_magnetic_iterate': (i32, [vp, ctypes.POINTER(MagneticBuffers), vp, i32, i32, vp]),
         'mmx_curl_ft': (i32, [vp, vp, vp, vp]),
         'mmx_green_ft': (i32, [vp, vp, dbl, dbl, vp]),
         'mmx_chi_mix': (i32, [vp, vp, vp, vp, vp, vp, ctypes.POINTER(dbl), vp, vp, i64, i32, vp]),

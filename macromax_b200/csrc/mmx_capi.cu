@@ -182,7 +182,10 @@ size_t word_bytes(int prec) { return prec == MMX_C128 ? 16 : 8; }
 
 // Pencils per tile: as many as fit ~64 KB of shared memory (at least 4 consecutive strided pencils, i.e. one
 // 32-byte sector per row, when the row fits), bounded by the 512-thread launch bound of the pass kernels.
-void choose_tile(const FFTAxis& ax, int C, int64_t outer, int64_t inner, int prec, PassCfg& pc) {
+// min_tiles > 0: narrow the tile (down to 4 pencils on a strided axis, 1 on the contiguous one) until the pass has
+// at least that many tiles, so that small transforms still spread over the SMs
+void choose_tile(const FFTAxis& ax, int C, int64_t outer, int64_t inner, int prec, PassCfg& pc,
+                 int64_t min_tiles = 0) {
   const size_t wb = word_bytes(prec);
   const size_t budget = 64 * 1024;
   const int64_t npenc = outer * inner;
@@ -199,6 +202,8 @@ void choose_tile(const FFTAxis& ax, int C, int64_t outer, int64_t inner, int pre
     P = 1;
     while (P * 2 <= pmax && smem_of(P * 2) <= budget && thr_of(P * 2) <= 512) P *= 2;
   }
+  const int pfloor = inner > 1 ? (int)std::min<int64_t>(inner, 4) : 1;
+  while (min_tiles > 0 && P / 2 >= pfloor && (npenc + P - 1) / P < min_tiles) P /= 2;
   pc.P = P;
   pc.sP = P > 1 ? P + 1 : 1;
   int thr = thr_of(P);
@@ -722,7 +727,7 @@ template <class R> int run_fftn(mmx_plan* p, const void* in, void* out, int64_t 
     for (int i = 0; i < axis; ++i) outer *= p->shape[i];
     for (int i = axis + 1; i < d; ++i) inner *= p->shape[i];
     PassCfg pc;
-    choose_tile(p->ax[axis], 1, outer, inner, p->prec, pc);
+    choose_tile(p->ax[axis], 1, outer, inner, p->prec, pc, 2 * (int64_t)sm_count());
     FFTPassArgs<R> a;
     a.ax = p->ax[axis];
     a.outer = outer;
@@ -1191,10 +1196,10 @@ extern "C" int mmx_green_ft(mmx_plan* p, void* F, double alpha_re, double alpha_
   const int blocks = grid_blocks(p->N, 256);
   if (p->prec == MMX_C128)
     k_green_ft<double><<<blocks, 256, 0, s>>>((double2*)F, g, kv_of<double>(p, 0), kv_of<double>(p, 1),
-                                              kv_of<double>(p, 2), alpha_re, alpha_im);
+                                              kv_of<double>(p, 2), alpha_re, alpha_im, nullptr);
   else
     k_green_ft<float><<<blocks, 256, 0, s>>>((float2*)F, g, kv_of<float>(p, 0), kv_of<float>(p, 1),
-                                             kv_of<float>(p, 2), (float)alpha_re, (float)alpha_im);
+                                             kv_of<float>(p, 2), (float)alpha_re, (float)alpha_im, nullptr);
   MMX_CUDA(cudaGetLastError());
   return MMX_OK;
 }
@@ -1211,12 +1216,12 @@ extern "C" int mmx_chi_mix(const void* x, const void* d, const void* chi_ee, con
     auto c = [&](int i) { return make_double2(coef[2 * i], coef[2 * i + 1]); };
     k_chi_mix<double><<<blocks, 256, 0, s>>>((const double2*)x, (const double2*)d, (const double2*)chi_ee,
                                              (const double2*)chi_eh, (const double2*)chi_he, (const double2*)chi_hh,
-                                             c(0), c(1), c(2), c(3), c(4), (double2*)u, (double2*)w, nvox);
+                                             c(0), c(1), c(2), c(3), c(4), (double2*)u, (double2*)w, nvox, nullptr);
   } else {
     auto c = [&](int i) { return make_float2((float)coef[2 * i], (float)coef[2 * i + 1]); };
     k_chi_mix<float><<<blocks, 256, 0, s>>>((const float2*)x, (const float2*)d, (const float2*)chi_ee,
                                             (const float2*)chi_eh, (const float2*)chi_he, (const float2*)chi_hh,
-                                            c(0), c(1), c(2), c(3), c(4), (float2*)u, (float2*)w, nvox);
+                                            c(0), c(1), c(2), c(3), c(4), (float2*)u, (float2*)w, nvox, nullptr);
   }
   MMX_CUDA(cudaGetLastError());
   return MMX_OK;
@@ -1236,6 +1241,101 @@ extern "C" int mmx_axpby(void* out, const void* x, const void* y, double a_re, d
                                           make_float2((float)a_re, (float)a_im), make_float2((float)b_re, (float)b_im),
                                           nwords);
   MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+namespace {
+// niter iterations of the magnetic split-Richardson iteration with the decisions on the device (mmx_magnetic.cuh)
+template <class R>
+int run_magnetic(mmx_plan* p, const mmx_magnetic_buffers* b, mmx_rhs_state* st, int niter, cudaStream_t s) {
+  using C = cpx<R>;
+  const int64_t N = p->N, n3 = 3 * N;
+  const KGrid g = kgrid_of(p);
+  const R *k0 = kv_of<R>(p, 0), *k1 = kv_of<R>(p, 1), *k2 = kv_of<R>(p, 2);
+  C* E = (C*)b->E;
+  const C* src = (const C*)b->src;
+  const C *ee = (const C*)b->chi_ee, *eh = (const C*)b->chi_eh, *he = (const C*)b->chi_he, *hh = (const C*)b->chi_hh;
+  C *t = (C*)b->work[0], *u = (C*)b->work[1], *w = (C*)b->work[2], *dx = (C*)b->work[3], *d = (C*)b->work[4];
+  C *F = (C*)b->work[5], *G = (C*)b->work[6];
+  const int bv = grid_blocks(N, 256), b3 = grid_blocks(n3, 256);
+  const int nb = (int)std::min<int64_t>(b3, p->partials_len / 3);
+  const C zero = mkc<R>((R)0, (R)0);
+  auto curl = [&](const C* x, C* out) -> int {  // out = IFFT(i k x FFT(x))
+    int rc = run_fftn<R>(p, x, F, 3, 0, s);
+    if (rc != MMX_OK) return rc;
+    k_curl_ft<R><<<bv, 256, 0, s>>>(F, G, g, k0, k1, k2);
+    MMX_CUDA(cudaGetLastError());
+    return run_fftn<R>(p, G, out, 3, 1, s);
+  };
+  auto chi_head = [&](const C* x) -> int {  // u = chi_EE x + chi_HE Dx, dx = D (chi_EH x + chi_HH Dx)
+    int rc = curl(x, dx);
+    if (rc != MMX_OK) return rc;
+    k_chi_mix<R><<<bv, 256, 0, s>>>(x, dx, ee, eh, he, hh, zero, zero, zero, zero, zero, u, w, N, st);
+    MMX_CUDA(cudaGetLastError());
+    return curl(w, dx);
+  };
+  for (int it = 0; it < niter; ++it) {
+    int rc = chi_head(E);
+    if (rc != MMX_OK) return rc;
+    k_mag_sum_src<R><<<b3, 256, 0, s>>>(t, u, dx, src, st, n3);
+    if ((rc = run_fftn<R>(p, t, F, 3, 0, s)) != MMX_OK) return rc;
+    k_green_ft<R><<<bv, 256, 0, s>>>(F, g, k0, k1, k2, (R)0, (R)1, st);
+    if ((rc = run_fftn<R>(p, F, t, 3, 1, s)) != MMX_OK) return rc;
+    k_axpby<R><<<b3, 256, 0, s>>>(t, t, E, mkc<R>((R)1, (R)0), mkc<R>((R)-1, (R)0), n3);
+    if ((rc = chi_head(t)) != MMX_OK) return rc;
+    k_mag_update<R><<<nb, 256, 0, s>>>(d, u, dx, E, n3, p->partials);
+    k_mag_decide<<<1, 256, 0, s>>>(p->partials, nb, st);
+    k_mag_accept<R><<<b3, 256, 0, s>>>(E, d, st, n3);
+    MMX_CUDA(cudaGetLastError());
+  }
+  return MMX_OK;
+}
+}  // namespace
+
+extern "C" int mmx_magnetic_iterate(mmx_plan* p, const mmx_magnetic_buffers* b, mmx_rhs_state* st, int niter,
+                                    int use_graph, void* stream) {
+  if (!p || !b || !st || !b->E || !b->src || !b->chi_ee || !b->chi_eh || !b->chi_he || !b->chi_hh)
+    return fail(MMX_ERR_ARG, "NULL plan or buffer");
+  for (int i = 0; i < 7; ++i)
+    if (!b->work[i]) return fail(MMX_ERR_ARG, "NULL work buffer");
+  if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
+  if (p->batch != 1 || p->ncomp != 1) return fail(MMX_ERR_ARG, "the plan must be a 1-component, 1-batch plan");
+  if (niter < 1) return fail(MMX_ERR_ARG, "niter must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!use_graph)
+    return p->prec == MMX_C128 ? run_magnetic<double>(p, b, st, niter, s) : run_magnetic<float>(p, b, st, niter, s);
+  GraphKey key;
+  key.ptrs = {(const void*)p, b->E, b->src, b->chi_ee, b->chi_eh, b->chi_he, b->chi_hh, (const void*)st};
+  for (int i = 0; i < 7; ++i) key.ptrs.push_back(b->work[i]);
+  key.ints = {-3, niter};  // -3: a magnetic iteration chunk
+  cudaGraphExec_t exec = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_graph_mutex);
+    for (const GraphEntry& ge : g_graphs)
+      if (ge.key == key) exec = ge.exec;
+  }
+  if (!exec) {
+    cudaStream_t cs = nullptr;
+    MMX_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    int rc = e == cudaSuccess ? MMX_OK : cuda_fail(e, "cudaStreamBeginCapture");
+    if (rc == MMX_OK) {
+      rc = p->prec == MMX_C128 ? run_magnetic<double>(p, b, st, niter, cs) : run_magnetic<float>(p, b, st, niter, cs);
+      e = cudaStreamEndCapture(cs, &graph);
+      if (rc == MMX_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
+    }
+    if (rc == MMX_OK) {
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate");
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    if (rc != MMX_OK) return rc;
+    std::lock_guard<std::mutex> lock(g_graph_mutex);
+    g_graphs.push_back(GraphEntry{key, exec});
+  }
+  MMX_CUDA(cudaGraphLaunch(exec, s));
   return MMX_OK;
 }
 

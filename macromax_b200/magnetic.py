@@ -9,11 +9,11 @@ spatial frequency over k0), and alpha_i is that sum; then the kernel-width bias 
 
 Iteration (solver.py:1064-1098 with chi_op of solver.py:531-552):
     d = chi[G(chi E + s') - E],   chi(x) = chi_EE x + chi_HE D x + D(chi_EH x + chi_HH D x),   D = i k x
-composed of device kernels: batched FFTs (mmx_fftn), the spectral curl (mmx_curl_ft), the dyadic Green multiply
-(mmx_green_ft), the 3x3 block products (mmx_chi_mix) and linear combinations (mmx_axpby); FP64 norms (mmx_norm).
-The four blocks and s' stay at their set-up alpha0: a divergence-guard rejection (alpha_i x 1.5) only changes the
-complex scale factors passed to mmx_chi_mix (solver.py:514-528).  The accept / reject decision is taken on the host
-after each iteration, as in the reference loop.
+run by mmx_magnetic_iterate: batched FFTs, the spectral curl, the dyadic Green multiply, the 3x3 block products and
+a fused update that also accumulates the FP64 norms.  The four blocks and s' stay at their set-up alpha0: a
+divergence-guard rejection (alpha_i x 1.5) only changes the scale factors the kernels derive from the right-hand
+side's device state (solver.py:514-528).  The accept / reject decision and the stop rule are taken on the device, so
+a chunk of iterations replays from one CUDA graph without a host round trip.
 """
 from __future__ import annotations
 
@@ -215,7 +215,6 @@ class MagneticSolution:
         self._pre = MagneticPreconditioner(epsilon, func2arr(xi), func2arr(zeta), mu, grid.step, self._wavenumber,
                                            self._bound.thickness, float(np.finfo(self._dtype).eps))
         self._alpha0 = self._pre.alpha
-        self._alpha = self._pre.alpha
         self._device = torch.device(device if device is not None else 'cuda')
         N = grid.size
         self._N = N
@@ -235,13 +234,37 @@ class MagneticSolution:
             def field():
                 return torch.zeros((3, N), dtype=self._tdtype, device=self._device)
 
-            self._E, self._t, self._u, self._w, self._dx, self._d = (field() for _ in range(6))
-            self._F, self._G, self._src = field(), field(), field()
-            self._norm_dev = torch.zeros(1, dtype=torch.float64, device=self._device)
+            self._E, self._src = field(), field()
+            self._work = [field() for _ in range(7)]
+            self._state = torch.zeros(nat.STATE_DTYPE.itemsize, dtype=torch.uint8, device=self._device)
+        self._buffers = nat.MagneticBuffers(
+            E=nat.device_ptr(self._E), src=nat.device_ptr(self._src), chi_ee=nat.device_ptr(self._ee),
+            chi_eh=nat.device_ptr(self._eh), chi_he=nat.device_ptr(self._he), chi_hh=nat.device_ptr(self._hh),
+            work=(nat.ctypes.c_void_p * 7)(*[t.data_ptr() for t in self._work]))
+        st = np.zeros(1, dtype=nat.STATE_DTYPE)
+        st['alpha_re'] = st['alpha0_re'] = self._alpha0.real
+        st['alpha_im'] = st['alpha0_im'] = self._alpha0.imag
+        st['prev_norm'] = inf
+        st['rtol'] = -1.0
+        st['maxiter'] = inf
+        st['active'] = 1
+        self._write_state(st)
         self.source_distribution = source_distribution
         self.E = initial_field
-        self._iteration = 0
-        self._rejections = 0
+
+    # -- device state (mmx_rhs_state) --------------------------------------------------------------------------------
+    def _read_state(self) -> np.ndarray:
+        return self._state.cpu().numpy().view(nat.STATE_DTYPE).copy()
+
+    def _write_state(self, st: np.ndarray):
+        raw = np.ascontiguousarray(st, dtype=nat.STATE_DTYPE).view(np.uint8)
+        self._state.copy_(torch.from_numpy(raw.copy()).to(self._device))
+
+    def _set_state(self, **values):
+        st = self._read_state()
+        for k, v in values.items():
+            st[k] = v
+        self._write_state(st)
 
     # -- properties of the reference Solution ------------------------------------------------------------------------
     @property
@@ -278,7 +301,8 @@ class MagneticSolution:
 
     @property
     def alpha(self) -> complex:
-        return self._alpha
+        st = self._read_state()[0]
+        return complex(st['alpha_re'], st['alpha_im'])
 
     @property
     def beta(self) -> float:
@@ -286,26 +310,29 @@ class MagneticSolution:
 
     @property
     def iteration(self) -> int:
-        return self._iteration
+        return int(self._read_state()[0]['iteration'])
 
     @iteration.setter
     def iteration(self, it: int = 0):
-        self._iteration = int(it)
+        self._set_state(iteration=int(it))
 
     @property
     def previous_update_norm(self) -> float:
         """solver.py:1018-1024: in field units (the stored field is E k0^2)."""
-        return float(self._prev / self._wavenumber ** 2)
+        return float(self._read_state()[0]['prev_norm'] / self._wavenumber ** 2)
 
     @property
     def rejections(self) -> int:
-        return self._rejections
+        return int(self._read_state()[0]['rejections'])
 
     @property
     def residue(self) -> float:
-        """solver.py:1026-1042: the last accepted update norm over the field norm."""
-        e = self._norm(self._E)
-        return self._prev / e if e > 0 and np.isfinite(self._prev) else (0.0 if self._prev == 0 else inf)
+        """solver.py:1026-1042: the last accepted update norm over the field norm (as of the last iteration)."""
+        st = self._read_state()[0]
+        prev = float(st['prev_norm'])
+        if not np.isfinite(prev):
+            return inf
+        return float(st['residue'])
 
     @property
     def source_distribution(self) -> np.ndarray:
@@ -318,7 +345,7 @@ class MagneticSolution:
         s = np.broadcast_to(_matrix_field(s, self._grid.ndim)[:, 0], (3, *self._grid.shape))
         self._src.copy_(torch.from_numpy(np.ascontiguousarray(s * self._pre.source_scale, dtype=self._dtype))
                         .reshape(3, -1).to(self._device))
-        self._prev = inf
+        self._set_state(prev_norm=inf)
 
     @property
     def E(self) -> np.ndarray:
@@ -329,83 +356,46 @@ class MagneticSolution:
     def E(self, E):
         E = np.broadcast_to(np.asarray(E), (3, *self._grid.shape)) * self._wavenumber ** 2
         self._E.copy_(torch.from_numpy(np.ascontiguousarray(E, dtype=self._dtype)).reshape(3, -1).to(self._device))
-        self._prev = inf
-
-    # -- device operators --------------------------------------------------------------------------------------------
-    def _stream(self):
-        import ctypes
-        s = torch.cuda.current_stream(self._device).cuda_stream
-        return ctypes.c_void_p(s) if s else None
-
-    def _norm(self, t) -> float:
-        nat.call('mmx_norm', self._plan.handle, nat.device_ptr(t), t.numel(), self._precision,
-                 nat.device_ptr(self._norm_dev), self._stream())
-        return float(self._norm_dev.item())
-
-    def _axpby(self, out, x, y, a, b):
-        a, b = complex(a), complex(b)
-        nat.call('mmx_axpby', nat.device_ptr(out), nat.device_ptr(x), nat.device_ptr(y), a.real, a.imag, b.real,
-                 b.imag, out.numel(), self._precision, self._stream())
-
-    def _curl(self, x, out):
-        """out = D x = IFFT(i k x FFT(x))."""
-        p, s = self._plan.handle, self._stream()
-        nat.call('mmx_fftn', p, nat.device_ptr(x), nat.device_ptr(self._F), 3, 0, s)
-        nat.call('mmx_curl_ft', p, nat.device_ptr(self._F), nat.device_ptr(self._G), s)
-        nat.call('mmx_fftn', p, nat.device_ptr(self._G), nat.device_ptr(out), 3, 1, s)
-
-    def _coef(self):
-        """chi(alpha) from the blocks at alpha0 (solver.py:514-528): EE = f EE0 + i (alpha0 - alpha) / alpha_i I,
-        the other blocks and s' scaled by f = alpha0_i / alpha_i."""
-        import ctypes
-        a0, a = self._alpha0, self._alpha
-        f = a0.imag / a.imag
-        ee_b = 1.0j * (a0 - a) / a.imag
-        vals = [f, 0.0, ee_b.real, ee_b.imag, f, 0.0, f, 0.0, f, 0.0]
-        return (ctypes.c_double * 10)(*vals)
-
-    def _chi_op(self, x, out):
-        self._curl(x, self._dx)
-        nat.call('mmx_chi_mix', nat.device_ptr(x), nat.device_ptr(self._dx), nat.device_ptr(self._ee),
-                 nat.device_ptr(self._eh), nat.device_ptr(self._he), nat.device_ptr(self._hh), self._coef(),
-                 nat.device_ptr(self._u), nat.device_ptr(self._w), self._N, self._precision, self._stream())
-        self._curl(self._w, self._dx)
-        self._axpby(out, self._u, self._dx, 1.0, 1.0)
-
-    def _update(self):
-        """d = chi [G (chi E + s') - E] into self._d."""
-        p, s = self._plan.handle, self._stream()
-        self._chi_op(self._E, self._t)
-        self._axpby(self._t, self._t, self._src, 1.0, self._alpha0.imag / self._alpha.imag)
-        nat.call('mmx_fftn', p, nat.device_ptr(self._t), nat.device_ptr(self._F), 3, 0, s)
-        nat.call('mmx_green_ft', p, nat.device_ptr(self._F), self._alpha.real, self._alpha.imag, s)
-        nat.call('mmx_fftn', p, nat.device_ptr(self._F), nat.device_ptr(self._t), 3, 1, s)
-        self._axpby(self._t, self._t, self._E, 1.0, -1.0)
-        self._chi_op(self._t, self._d)
+        self._set_state(prev_norm=inf)
 
     # -- iteration ---------------------------------------------------------------------------------------------------
+    def _run(self, niter: int):
+        import ctypes
+        stream = torch.cuda.current_stream(self._device).cuda_stream
+        nat.call('mmx_magnetic_iterate', self._plan.handle, ctypes.byref(self._buffers),
+                 nat.device_ptr(self._state), int(niter), 1, ctypes.c_void_p(stream) if stream else None)
+
+    def _check(self, st):
+        if int(st['status']) == nat.MMX_STATUS_ZERODIV:
+            raise ZeroDivisionError('float division by zero')
+
     def __iter__(self):
+        """solver.py:1049-1098: every next() runs one iteration on the device."""
+        self._set_state(rtol=-1.0, maxiter=inf, active=1, status=0)
         while True:
-            self._iteration += 1
-            self._update()
-            nu = self._norm(self._d)
-            if self._prev == 0.0:
-                raise ZeroDivisionError('float division by zero')
-            if nu / self._prev < 1.0:
-                self._axpby(self._E, self._E, self._d, 1.0, 1.0)
-                self._prev = nu
-            else:  # solver.py:1090-1094
-                self._alpha = complex(self._alpha.real, 1.5 * self._alpha.imag)
-                self._rejections += 1
+            self._run(1)
+            self._check(self._read_state()[0])
             yield self
 
-    def solve(self, callback=None, rtol: float = 0, maxiter=inf):
-        if callback is None:
-            def callback(sol):
-                return sol.iteration < maxiter and sol.residue > rtol
-        for sol in self:
-            if not callback(sol):
+    def solve(self, callback=None, rtol: float = 0, maxiter=inf, chunk: int = 8, max_chunk: int = 64):
+        """solver.py:1100-1123.  With no callback (or the reference's default one) the stop rule runs on the device
+        in chunks of iterations; any other callback is called after every iteration."""
+        from .solver import _default_callback
+        if callback is _default_callback:
+            callback, rtol, maxiter = None, 1e-4, 1e4
+        if callback is not None:
+            for sol in self:
+                if not callback(sol):
+                    break
+            return self
+        self._set_state(rtol=float(rtol), maxiter=float(maxiter), active=1, status=0)
+        while True:
+            self._run(chunk)
+            st = self._read_state()[0]
+            self._check(st)
+            if not st['active']:
                 break
+            chunk = min(2 * chunk, max_chunk)
         return self
 
     def close(self):

@@ -116,7 +116,7 @@ class DeviceSetup:
         self.nvox = int(np.prod(shape))
         dev = torch.device(device if device is not None else 'cuda')
         m = np.ascontiguousarray(np.broadcast_to(eps_field, (3, 3, *shape)).reshape(9, self.nvox), np.complex128)
-        self.M = torch.from_numpy(m).to(dev)
+        self.M = torch.from_numpy(np.require(m, requirements='W')).to(dev)  # a read-only view is copied first
         self.out = torch.zeros(2, dtype=torch.float64, device=dev)
         with torch.cuda.device(dev):
             self.plan = nat.Plan((8,) * max(1, min(ndim, 1)), 1, 1, nat.MMX_C128)

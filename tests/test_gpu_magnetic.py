@@ -51,6 +51,21 @@ def test_magnetic_complex64():
             break
 
 
+@pytest.mark.parametrize('dtype', [np.complex64, np.complex128])
+def test_device_stop_rule_equals_per_iteration_loop(dtype):
+    """solve() with a tolerance runs chunks of iterations with the stop rule on the device (the chunks may pass the
+    stopping iteration: those iterations leave E and the state unchanged).  It stops at the same iteration as the
+    Python callback loop, with the same field, alpha and rejections."""
+    z = load_golden('magnetic2d_48_c128')
+    a, b = _solution(z, dtype), _solution(z, dtype)
+    rtol = 1e-3
+    a.solve(None, rtol=rtol, maxiter=1e4)
+    b.solve(lambda s: s.iteration < 1e4 and s.residue > rtol)
+    assert a.iteration == b.iteration and a.residue <= rtol < 1.0
+    assert a.rejections == b.rejections and a.alpha == b.alpha
+    assert np.array_equal(a.E, b.E)
+
+
 def test_reference_negative_index_plate_known_answer():
     """The reference's magnetic solve: a -1.5 index plate, 128^2 grid, complex64, to residue 1e-3 in at most 1000
     iterations, with the field norms in front of and behind the plate that its test asserts to 5 decimals."""
