@@ -15,6 +15,7 @@
 #include "mmx_plane.cuh"
 #include "mmx_epro.cuh"
 #include "mmx_magnetic.cuh"
+#include "mmx_fftr.cuh"
 
 #define MMX_ABI_VERSION 1
 
@@ -718,14 +719,81 @@ int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kin
   return MMX_OK;
 }
 
+// Register-staged FFT-only pass (mmx_fftr.cuh) for one axis of mmx_fftn: false if this axis has none (then the
+// runtime-radix pass runs).  Contiguous axis: PC rows per tile, the default tile when that gives two waves of tiles,
+// else a quarter of it.
+template <int DIR, int N>
+bool fftr_axis_n(const float2* in, float2* out, int64_t outer, int64_t inner, const float2* tw, float scale,
+                 cudaStream_t s, cudaError_t* err) {
+  if (inner > 1) {
+    if (inner % kRegP != 0 || scale != 1.0f) return false;
+    const int64_t tiles = outer * inner / kRegP;
+    const size_t smem = ((size_t)N * kRegP + N) * sizeof(float2);
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured_mask & (1 << dev))) {  // 512-sample tiles need more than the default 48 KiB
+      cudaFuncSetAttribute(k_fftr_strided<DIR, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap);
+      configured_mask |= (1 << dev);
+    }
+    k_fftr_strided<DIR, N><<<(unsigned)tiles, RegThreads<1, N>::value, smem, s>>>(in, out, inner, tw);
+    *err = cudaGetLastError();
+    return true;
+  }
+  constexpr int PCB = RegCDefault<1, N>::PC;
+  constexpr int PCS = PCB >= 4 ? PCB / 4 : 1;
+  const int64_t rows = outer;
+  if (rows % PCB == 0 && rows / PCB >= 2 * (int64_t)sm_count()) {
+    const size_t smem = ((size_t)PCB * RegC<1, N, PCB>::PITCH + N) * sizeof(float2);
+    k_fftr_contig<DIR, N, PCB><<<(unsigned)(rows / PCB), RegC<1, N, PCB>::THREADS, smem, s>>>(in, out, tw, scale);
+  } else if (rows % PCS == 0) {
+    const size_t smem = ((size_t)PCS * RegC<1, N, PCS>::PITCH + N) * sizeof(float2);
+    k_fftr_contig<DIR, N, PCS><<<(unsigned)(rows / PCS), RegC<1, N, PCS>::THREADS, smem, s>>>(in, out, tw, scale);
+  } else {
+    return false;
+  }
+  *err = cudaGetLastError();
+  return true;
+}
+
+template <int DIR>
+bool fftr_axis(int n, const float2* in, float2* out, int64_t outer, int64_t inner, const float2* tw, float scale,
+               cudaStream_t s, cudaError_t* err) {
+  switch (n) {
+    case 64: return fftr_axis_n<DIR, 64>(in, out, outer, inner, tw, scale, s, err);
+    case 128: return fftr_axis_n<DIR, 128>(in, out, outer, inner, tw, scale, s, err);
+    case 256: return fftr_axis_n<DIR, 256>(in, out, outer, inner, tw, scale, s, err);
+    case 512: return fftr_axis_n<DIR, 512>(in, out, outer, inner, tw, scale, s, err);
+    default: return false;
+  }
+}
+
 template <class R> int run_fftn(mmx_plan* p, const void* in, void* out, int64_t nbatch, int inverse, cudaStream_t s) {
   const int d = p->ndim;
   const void* cur_in = in;
+  // the inverse's 1 / N is applied once, by the first (contiguous-axis) pass: to its input in the register-staged
+  // pass, to its output in the runtime-radix one
   for (int k = 0; k < d; ++k) {
     const int axis = d - 1 - k;  // contiguous axis first
     int64_t outer = nbatch, inner = 1;
     for (int i = 0; i < axis; ++i) outer *= p->shape[i];
     for (int i = axis + 1; i < d; ++i) inner *= p->shape[i];
+    if constexpr (std::is_same<R, float>::value) {
+      if (!p->force_generic) {
+        const float sc = (inverse && k == 0) ? (float)(1.0 / (double)p->N) : 1.0f;
+        cudaError_t e = cudaSuccess;
+        const float2* tw = (const float2*)p->ax[axis].tw;
+        const bool ran = inverse ? fftr_axis<+1>(p->ax[axis].n, (const float2*)cur_in, (float2*)out, outer, inner, tw,
+                                                 sc, s, &e)
+                                 : fftr_axis<-1>(p->ax[axis].n, (const float2*)cur_in, (float2*)out, outer, inner, tw,
+                                                 sc, s, &e);
+        if (ran) {
+          if (e != cudaSuccess) return cuda_fail(e, "register-staged FFT pass");
+          cur_in = out;
+          continue;
+        }
+      }
+    }
     PassCfg pc;
     choose_tile(p->ax[axis], 1, outer, inner, p->prec, pc, 2 * (int64_t)sm_count());
     FFTPassArgs<R> a;
@@ -736,7 +804,7 @@ template <class R> int run_fftn(mmx_plan* p, const void* in, void* out, int64_t 
     a.sP = pc.sP;
     a.in = (const cpx<R>*)cur_in;
     a.out = (cpx<R>*)out;
-    a.scale = (R)((inverse && k == d - 1) ? 1.0 / (double)p->N : 1.0);
+    a.scale = (R)((inverse && k == 0) ? 1.0 / (double)p->N : 1.0);
     if (inverse) {
       auto kern = k_fft_pass<R, +1>;
       MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));

@@ -6,7 +6,10 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(5, 10, 20), (64,), (1024,), (128, 96), (16, 24, 20), (12, 7, 13), (30, 64), (256, 256), (3, 11)]
+# the last six take the register-staged passes on some or all axes (lengths 64 .. 512), alone or mixed with the
+# runtime-radix passes, with small and large contiguous tiles
+SHAPES = [(5, 10, 20), (64,), (1024,), (128, 96), (16, 24, 20), (12, 7, 13), (30, 64), (256, 256), (3, 11),
+          (128, 128), (64, 64, 64), (512, 256), (32, 256), (256, 30), (16, 128, 512)]
 
 
 def _ptr(t):
