@@ -134,6 +134,20 @@ def cpu_oracle_rate(wl, dtype, iters: int, workers: int):
     return int(np.prod(wl['shape'])) * iters / dt, dt
 
 
+def cpu_torch_rate(wl, dtype, iters: int):
+    """The same iteration with torch CPU tensors (the reference's torch backend form): voxel-iterations/s."""
+    import torch
+    from oracle import mmoracle as mo
+    from oracle.torch_cpu import TorchCPUIteration
+    it = TorchCPUIteration(mo.from_workload(wl, dtype))
+    it.advance()  # warm-up iteration
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        it.advance()
+    dt = time.perf_counter() - t0
+    return int(np.prod(wl['shape'])) * iters / dt, dt, torch.get_num_threads()
+
+
 def bench_reference(args, wl, rank, world, pg):
     """--impl reference: the oracle's iteration on the host cores, one iteration per step."""
     dtype = np.complex64
@@ -247,6 +261,11 @@ def bench_ours(args, wl, rank, world, local, pg):
         cpu = {'value': rate, 'unit': UNIT, 'cores': os.cpu_count() or 1, 'kind': 'port',
                'sample': f'{args.cpu_iters} iterations of the numpy oracle on the full workload ({dt:.1f} s), '
                          f'scipy.fft with {os.cpu_count()} workers'}
+        if np.asarray(wl['epsilon']).ndim == len(wl['shape']):  # isotropic: the torch-CPU form as well
+            trate, tdt, threads = cpu_torch_rate(wl, dtype, args.cpu_iters)
+            cpu['torch_cpu'] = {'value': trate, 'unit': UNIT, 'cores': threads, 'kind': 'port',
+                                'sample': f'{args.cpu_iters} iterations with torch CPU tensors on the full workload '
+                                          f'({tdt:.1f} s), {threads} threads'}
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,

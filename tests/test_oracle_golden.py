@@ -107,3 +107,17 @@ def test_magnetic_oracle_matches_reference(name):
         g = z[f'E{it}']
         assert np.linalg.norm(rec[it] - g) <= 1e-13 * np.linalg.norm(g), it
     assert ref.alpha == complex(z['alpha_final'])
+
+
+@pytest.mark.parametrize('case', ['spheres3d', 'disks2d'])
+def test_torch_cpu_form_matches_numpy_oracle(case):
+    """The torch-CPU restatement timed beside the numpy oracle (bench.py cpu_baseline) takes the same steps."""
+    from macromax_b200 import workloads
+    from oracle import mmoracle as mo
+    from oracle.torch_cpu import TorchCPUIteration
+    wl = workloads.spheres_3d(n=16, nb_spheres=6) if case == 'spheres3d' else workloads.disks_2d(n=32)
+    ref = mo.from_workload(wl, np.complex128)
+    tc = TorchCPUIteration(mo.from_workload(wl, np.complex128))
+    for _ in range(8):
+        assert ref.advance() and tc.advance()
+        assert np.linalg.norm(tc.E.numpy() - ref.field) <= 1e-12 * np.linalg.norm(ref.field)
