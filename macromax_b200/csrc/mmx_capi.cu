@@ -87,6 +87,8 @@ struct PassCfg {
 };
 
 bool reg_length(int n, int C) { return C == 3 ? (n == 64 || n == 128) : (n == 64 || n == 128 || n == 256 || n == 512); }
+// the strided (middle) passes also take 192-sample vector pencils
+bool reg_strided_length(int n, int C) { return reg_length(n, C) || (C == 3 && n == 192); }
 
 constexpr int kFastP = 8;
 bool fast_length(int n) { return n == 64 || n == 128 || n == 192 || n == 256 || n == 384 || n == 512; }
@@ -298,7 +300,7 @@ int launch_fast(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
 
 template <int C, int OPS, int N>
 int launch_reg(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
-  if constexpr ((C == 3 && N > 128) || N == 192 || N == 384) {
+  if constexpr ((C == 3 && N > 128 && N != 192) || (C == 1 && N == 192) || N == 384) {
     return fail(MMX_ERR_ARG, "internal: no register-staged kernel for this length");
   } else {
     auto kern = k_reg_pass<C, OPS, N>;
@@ -591,7 +593,7 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
           pc.rc_smem = ((size_t)p->ncomp * pcr * (n + n / 16) + n) * sizeof(float2);
         }
       }
-      if (strided_op && inner % kRegP == 0 && reg_length(n, p->ncomp) && !p->no_reg) {
+      if (strided_op && inner % kRegP == 0 && reg_strided_length(n, p->ncomp) && !p->no_reg) {
         pc.reg = 1;
         pc.P = kRegP;
         pc.sP = kRegP;

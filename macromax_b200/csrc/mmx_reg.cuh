@@ -17,6 +17,8 @@ template <> struct RegPlan<64> { using type = RegPlanList<8, 8>; static constexp
 template <> struct RegPlan<128> { using type = RegPlanList<16, 8>; static constexpr int TPP = 8; };
 template <> struct RegPlan<256> { using type = RegPlanList<16, 16>; static constexpr int TPP = 16; };
 template <> struct RegPlan<512> { using type = RegPlanList<8, 8, 8>; static constexpr int TPP = 32; };
+// 192 (vector fields, strided passes only: the 192^3 anisotropic grids): 8 x 8 x 3, 8 threads per pencil
+template <> struct RegPlan<192> { using type = RegPlanList<8, 8, 3>; static constexpr int TPP = 8; };
 
 constexpr int kRegP = 16;
 

@@ -30,6 +30,17 @@ def rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(np.asarray(b).ravel()))
 
 
+def _stacked_voronoi(axis):
+    """The 64^3 Voronoi medium repeated three times along one grid axis (192 samples there)."""
+    from macromax_b200 import workloads as w
+    wl = w.voronoi_3d(n=64, nb_grains=12, boundary_px=48)
+    eps = np.concatenate([wl['epsilon']] * 3, axis=2 + axis)
+    src = np.concatenate([wl['source']] + [np.zeros_like(wl['source'])] * 2, axis=1 + axis)
+    shape = list(wl['shape'])
+    shape[axis] *= 3
+    return {**wl, 'shape': tuple(shape), 'epsilon': eps, 'source': src}
+
+
 def _cases():
     from macromax_b200 import workloads as w
     return {
@@ -38,6 +49,9 @@ def _cases():
         'disks2d_128': lambda: w.disks_2d(n=128),
         'disks2d_256': lambda: w.disks_2d(n=256),
         'voronoi3d_64': lambda: w.voronoi_3d(n=64, nb_grains=12, boundary_px=48),
+        # anisotropic 3x3 eps with 192-sample strided axes (register-staged 8 x 8 x 3 pencils)
+        'voronoi_192x64x64': lambda: _stacked_voronoi(0),
+        'voronoi_64x192x64': lambda: _stacked_voronoi(1),
         'mixed_3d': lambda: {**w.design_3d(n=64), 'shape': (64, 40, 64),
                              'epsilon': w.design_3d(n=64)['epsilon'][:, :40, :],
                              'source': w.design_3d(n=64)['source'][:, :, :40, :]},
@@ -87,7 +101,8 @@ def _solution_env(wl, env):
                 os.environ[k] = v
 
 
-@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256', 'mixed_3d'])
+@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256', 'mixed_3d', 'voronoi_192x64x64',
+                                  'voronoi_64x192x64'])
 def test_register_staged_matches_shared_staged(name):
     """k_reg_pass (strided passes, 16-pencil tiles, global<->register first/last stages) vs k_fast_pass."""
     wl = _cases()[name]()
