@@ -32,6 +32,7 @@ extern "C" {
 
 #define MMX_CHI_SCALAR 1 /* isotropic susceptibility, one word per voxel */
 #define MMX_CHI_MAT3 9   /* 3x3 susceptibility tensor, nine words per voxel */
+#define MMX_CHI_SYM6 6   /* symmetric 3x3 tensor, six words per voxel: xx, xy, xz, yy, yz, zz */
 
 /* status codes of an mmx_rhs_state */
 #define MMX_STATUS_OK 0
@@ -109,7 +110,8 @@ int mmx_norm(mmx_plan* plan, const void* x, int64_t nwords, int precision, doubl
  * g (1 - P_L) + (i alpha_i / alpha) P_L for vector fields (solver.py:564-584; backend/__init__.py:606-649).
  * The current field of RHS b is buffer state[b].cur of (E0, E1); the update is written to the other buffer and the
  * two swap roles on acceptance.  A right-hand side whose state is inactive is skipped (convergence mask).
- * chi: chi_kind MMX_CHI_SCALAR or MMX_CHI_MAT3, shared by all right-hand sides.  All launches are asynchronous on
+ * chi: chi_kind MMX_CHI_SCALAR, MMX_CHI_MAT3 or MMX_CHI_SYM6 (a symmetric tensor stored as its six distinct
+ * entries), shared by all right-hand sides.  All launches are asynchronous on
  * `stream`; no host synchronisation happens inside.
  */
 int mmx_iterate(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,

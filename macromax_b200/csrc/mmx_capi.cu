@@ -511,6 +511,7 @@ template <int N>
 int fast_dispatch_n(const PassCfg& pc, const IterArgs<float>& a, int C, int chi_kind, int batch, cudaStream_t s) {
   if (C == 1) return fast_ops<1, MMX_CHI_SCALAR, N>(pc, a, batch, s);
   if (chi_kind == MMX_CHI_SCALAR) return fast_ops<3, MMX_CHI_SCALAR, N>(pc, a, batch, s);
+  if (chi_kind == MMX_CHI_SYM6) return fast_ops<3, MMX_CHI_SYM6, N>(pc, a, batch, s);
   return fast_ops<3, MMX_CHI_MAT3, N>(pc, a, batch, s);
 }
 
@@ -539,6 +540,7 @@ int dispatch_pass(const PassCfg& pc, const IterArgs<R>& a, int C, int chi_kind, 
     return dispatch_ops<R, 1, MMX_CHI_SCALAR>(pc, a, batch, s);
   }
   if (chi_kind == MMX_CHI_SCALAR) return dispatch_ops<R, 3, MMX_CHI_SCALAR>(pc, a, batch, s);
+  if (chi_kind == MMX_CHI_SYM6) return dispatch_ops<R, 3, MMX_CHI_SYM6>(pc, a, batch, s);
   return dispatch_ops<R, 3, MMX_CHI_MAT3>(pc, a, batch, s);
 }
 
@@ -1012,7 +1014,8 @@ int mmx_norm(mmx_plan* p, const void* x, int64_t nwords, int precision, double* 
 int mmx_iterate(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
                 mmx_rhs_state* state, int niter, void* stream) {
   if (!p || !E0 || !E1 || !chi || !src || !state) return fail(MMX_ERR_ARG, "NULL plan or buffer");
-  if (chi_kind != MMX_CHI_SCALAR && chi_kind != MMX_CHI_MAT3) return fail(MMX_ERR_ARG, "unknown chi_kind");
+  if (chi_kind != MMX_CHI_SCALAR && chi_kind != MMX_CHI_MAT3 && chi_kind != MMX_CHI_SYM6)
+    return fail(MMX_ERR_ARG, "unknown chi_kind");
   if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
   if (niter < 0) return fail(MMX_ERR_ARG, "negative iteration count");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1147,7 +1150,8 @@ int iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E
   for (int i = 0; i < n; ++i) {
     mmx_plan* p = plans[i];
     if (!p || !E0[i] || !E1[i] || !chi[i] || !src[i] || !state[i]) return fail(MMX_ERR_ARG, "NULL plan or buffer");
-    if (chi_kind[i] != MMX_CHI_SCALAR && chi_kind[i] != MMX_CHI_MAT3) return fail(MMX_ERR_ARG, "unknown chi_kind");
+    if (chi_kind[i] != MMX_CHI_SCALAR && chi_kind[i] != MMX_CHI_MAT3 && chi_kind[i] != MMX_CHI_SYM6)
+      return fail(MMX_ERR_ARG, "unknown chi_kind");
     if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
     key.ptrs.insert(key.ptrs.end(), {(const void*)p, E0[i], E1[i], chi[i], src[i], (const void*)state[i]});
     key.ints.push_back(chi_kind[i]);

@@ -157,8 +157,8 @@ __global__ void __launch_bounds__(FastThreads<C, N, P>::value, 2) k_fast_pass(It
           v0[c] = make_float2(ev[c].x, ev[c].y);
           v1[c] = make_float2(ev[c].z, ev[c].w);
         }
-        apply_chi<R, 3, MMX_CHI_MAT3>(a.chi, N3, vox, cc, v0, o0);
-        apply_chi<R, 3, MMX_CHI_MAT3>(a.chi, N3, vox + 1, cc, v1, o1);
+        apply_chi<R, 3, CHI>(a.chi, N3, vox, cc, v0, o0);
+        apply_chi<R, 3, CHI>(a.chi, N3, vox + 1, cc, v1, o1);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           t0[c] = o0[c] + cc.s * make_float2(sv[c].x, sv[c].y);

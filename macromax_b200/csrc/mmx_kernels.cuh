@@ -94,6 +94,19 @@ __device__ __forceinline__ void apply_chi(const cpx<R>* __restrict__ chi, int64_
     const cpx<R> x = cc.a * chi[vox] + cc.b;
 #pragma unroll
     for (int c = 0; c < C; ++c) out[c] = x * v[c];
+  } else if constexpr (CHI == MMX_CHI_SYM6) {
+    // the six distinct entries are read once each (row-major position -> stored entry)
+    constexpr int K[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    cpx<R> m[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) m[k] = cc.a * chi[k * N + vox];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      cpx<R> acc = cc.b * v[r];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) acc += m[K[r * 3 + s]] * v[s];
+      out[r] = acc;
+    }
   } else {
 #pragma unroll
     for (int r = 0; r < 3; ++r) {

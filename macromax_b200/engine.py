@@ -82,6 +82,7 @@ class IterationEngine:
             self.chi_kind = nat.MMX_CHI_SCALAR if m == 1 else nat.MMX_CHI_MAT3
             self.chi = chi0.to(self.device, self.torch_dtype).contiguous()
             self.alpha0 = complex(alpha0)
+            self._pack_symmetric()
             return
         chi0 = np.asarray(chi0)
         m = chi0.shape[0] * chi0.shape[1]
@@ -93,6 +94,18 @@ class IterationEngine:
         self.chi_kind = nat.MMX_CHI_SCALAR if m == 1 else nat.MMX_CHI_MAT3
         self.chi = torch.from_numpy(np.array(full, dtype=self.np_dtype, order='C')).to(self.device)
         self.alpha0 = complex(alpha0)
+        self._pack_symmetric()
+
+    def _pack_symmetric(self):
+        """A 3x3 chi that equals its transpose (every reciprocal medium: a symmetric permittivity, as in the uniaxial
+        grains of the anisotropic workload) is kept as its six distinct entries (MMX_CHI_SYM6), so the prologue and
+        epilogue passes read 6 words per voxel instead of 9."""
+        if self.chi_kind != nat.MMX_CHI_MAT3:
+            return
+        c = self.chi
+        if torch.equal(c[1], c[3]) and torch.equal(c[2], c[6]) and torch.equal(c[5], c[7]):
+            self.chi = c[list(nat.SYM6_ROWS)].contiguous()
+            self.chi_kind = nat.MMX_CHI_SYM6
 
     def rebase_alpha(self, chi0: np.ndarray, alpha0: complex, sources0: np.ndarray | None = None):
         """Install a new material (chi at alpha0) and reset every RHS's alpha to alpha0."""

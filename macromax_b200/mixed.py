@@ -64,6 +64,14 @@ class MixedSolution:
                 # C order explicitly: a permittivity built as a strided view reshapes to a strided view too
                 self.chi64 = torch.from_numpy(np.ascontiguousarray(chi, dtype=np.complex128)).to(self.device)
             s0 = src.reshape(self.batch, self.ncomp, N) * (1.0j / pre.alpha.imag / pre.beta)
+            # a 3x3 chi equal to its transpose in FP64 is kept as its six distinct entries, as the inner
+            # iteration keeps its complex64 copy
+            self.chi64_kind = eng.chi_kind if eng.chi_kind == nat.MMX_CHI_SCALAR else nat.MMX_CHI_MAT3
+            c = self.chi64
+            if self.chi64_kind == nat.MMX_CHI_MAT3 and torch.equal(c[1], c[3]) and torch.equal(c[2], c[6]) \
+                    and torch.equal(c[5], c[7]):
+                self.chi64 = c[list(nat.SYM6_ROWS)].contiguous()
+                self.chi64_kind = nat.MMX_CHI_SYM6
             self.src64 = torch.from_numpy(np.ascontiguousarray(s0, dtype=np.complex128)).to(self.device)
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
             self._norm = torch.zeros(1, dtype=torch.float64, device=self.device)
@@ -88,7 +96,7 @@ class MixedSolution:
             st['active'] = (~done).astype(np.int32)
             st['status'] = 0
             eng.write_state(st)
-            nat.call('mmx_defect', self.plan64.handle, _ptr(self.x), _ptr(self.chi64), eng.chi_kind, _ptr(self.src64),
+            nat.call('mmx_defect', self.plan64.handle, _ptr(self.x), _ptr(self.chi64), self.chi64_kind, _ptr(self.src64),
                      _ptr(eng.state), _ptr(eng.sources), _stream())
             eng.iterate(1)  # first correction step: its update norm is ||d(x)||
             st = eng.read_state()

@@ -136,3 +136,24 @@ def test_persistent_pipeline_matches_single_tile_passes(name):
     assert np.array_equal(pipe.E, single.E)
     st = pipe._engine.read_state()
     assert int(st['status'][0]) == 0
+
+
+@pytest.mark.parametrize('dtype', [np.complex64, np.complex128])
+def test_symmetric_chi_six_entries_equals_nine(dtype):
+    """A symmetric 3x3 chi is stored as its six distinct entries (MMX_CHI_SYM6); the iteration equals the one on all
+    nine entries (MMX_CHI_MAT3) of the same tensor."""
+    import torch
+    from macromax_b200 import _native as nat
+    wl = _cases()['voronoi3d_64']()
+    eps = wl['epsilon']
+    wl['epsilon'] = (eps + eps.transpose(1, 0, *range(2, eps.ndim))) / 2  # exactly symmetric in FP64 as well
+    a, b = _solution(wl, dtype), _solution(wl, dtype)
+    ea, eb = a._engine, b._engine
+    assert ea.chi_kind == nat.MMX_CHI_SYM6 and ea.chi.shape[0] == 6
+    full = torch.empty((9, eb.N), dtype=eb.chi.dtype, device=eb.chi.device)
+    for k, row in enumerate((0, 1, 2, 1, 3, 4, 2, 4, 5)):
+        full[k] = eb.chi[row]
+    eb.chi, eb.chi_kind = full, nat.MMX_CHI_MAT3
+    a.solve(None, rtol=0, maxiter=20)
+    b.solve(None, rtol=0, maxiter=20)
+    assert rel(a.E, b.E) < (1e-6 if dtype == np.complex64 else 1e-13)

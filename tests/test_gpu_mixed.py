@@ -73,7 +73,7 @@ def test_mixed_anisotropic_strided_permittivity():
     st['active'] = 1
     eng.write_state(st)
     s = torch.cuda.current_stream().cuda_stream
-    nat.call('mmx_defect', ms.plan64.handle, nat.device_ptr(ms.x), nat.device_ptr(ms.chi64), eng.chi_kind,
+    nat.call('mmx_defect', ms.plan64.handle, nat.device_ptr(ms.x), nat.device_ptr(ms.chi64), ms.chi64_kind,
              nat.device_ptr(ms.src64), nat.device_ptr(eng.state), nat.device_ptr(eng.sources),
              ctypes.c_void_p(s) if s else None)
     dev = eng.sources.cpu().numpy().reshape(3, 1, *wl['shape'])
