@@ -180,8 +180,9 @@ def bench_reference(args, wl, rank, world, pg):
 
 def config_of(args, wl):
     c = 3 if np.asarray(wl['source']).ndim > len(wl['shape']) and np.asarray(wl['source']).shape[0] == 3 else 1
+    chi = 'isotropic chi' if np.asarray(wl['epsilon']).ndim == len(wl['shape']) else '3x3 anisotropic chi'
     return {'workload': f"{wl['name']}: {'x'.join(map(str, wl['shape']))} grid, {c}-component field, "
-                        f"isotropic chi, complex64, 1 RHS", 'grid': list(wl['shape']), 'components': c,
+                        f"{chi}, complex64, 1 RHS", 'grid': list(wl['shape']), 'components': c,
             'batch': 1, 'l2': 'working set > L2 (no flush needed)'}
 
 
@@ -198,7 +199,8 @@ def bench_ours(args, wl, rank, world, local, pg):
     eng = sol._engine
     nvox = eng.N
     c = eng.ncomp
-    m = 1 if eng.chi_kind == nat.MMX_CHI_SCALAR else 9
+    # stored chi words per voxel: 1, 6 (a symmetric 3x3, the algorithmic figure's m) or 9
+    m = {nat.MMX_CHI_SCALAR: 1, nat.MMX_CHI_SYM6: 6}.get(eng.chi_kind, 9)
     tuned = None
     if args.variant >= 0:
         from macromax_b200 import autotune
