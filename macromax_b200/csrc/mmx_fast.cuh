@@ -123,6 +123,16 @@ __global__ void __launch_bounds__(FastThreads<C, N, P>::value, 2) k_fast_pass(It
   constexpr int pstride_c = STRIDED ? 1 : N;    // address step between pencils (contiguous case)
   const cpx<R>* __restrict__ twg = (const cpx<R>*)a.ax.tw;
   for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  if constexpr (!STRIDED && (OPS & (OP_PRO | OP_EPI)) != 0) {
+    // the tile's P rows are contiguous chunks of chi, E (and s'): bring them into L2 in bulk while the first loads
+    // are in flight (the epilogue's T is still in L2 from the previous pass)
+    constexpr int M = CHI == MMX_CHI_SCALAR ? 1 : (CHI == MMX_CHI_SYM6 ? 6 : 9);
+    constexpr unsigned chunk = (unsigned)(P * N * sizeof(float2));
+    if (tid < M) prefetch_l2(a.chi + (int64_t)tid * N3 + tile_base, chunk);
+    else if (tid < M + C) prefetch_l2(Ecur + fbase + (int64_t)(tid - M) * N3 + tile_base, chunk);
+    else if ((OPS & OP_PRO) != 0 && tid < M + 2 * C)
+      prefetch_l2(a.src + fbase + (int64_t)(tid - M - C) * N3 + tile_base, chunk);
+  }
 
   // ---------------- load (16-byte accesses: two neighbouring words) ----------------
   // strided: pair = (pl, pl+1) at the same j; contiguous: pair = (j, j+1) of the same pencil
@@ -157,8 +167,7 @@ __global__ void __launch_bounds__(FastThreads<C, N, P>::value, 2) k_fast_pass(It
           v0[c] = make_float2(ev[c].x, ev[c].y);
           v1[c] = make_float2(ev[c].z, ev[c].w);
         }
-        apply_chi<R, 3, CHI>(a.chi, N3, vox, cc, v0, o0);
-        apply_chi<R, 3, CHI>(a.chi, N3, vox + 1, cc, v1, o1);
+        apply_chi2<3, CHI>(a.chi, N3, vox, cc, v0, v1, o0, o1);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           t0[c] = o0[c] + cc.s * make_float2(sv[c].x, sv[c].y);
@@ -291,8 +300,7 @@ __global__ void __launch_bounds__(FastThreads<C, N, P>::value, 2) k_fast_pass(It
         v0[c] = s0 - e0[c];
         v1[c] = s1 - e1[c];
       }
-      apply_chi<R, C, CHI>(a.chi, N3, vox, cc, v0, d0);
-      apply_chi<R, C, CHI>(a.chi, N3, vox + 1, cc, v1, d1);
+      apply_chi2<C, CHI>(a.chi, N3, vox, cc, v0, v1, d0, d1);
 #pragma unroll
       for (int c = 0; c < C; ++c) {
         const float2 n0 = e0[c] + d0[c], n1 = e1[c] + d1[c];

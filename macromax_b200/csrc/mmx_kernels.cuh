@@ -86,6 +86,11 @@ __device__ __forceinline__ int64_t pencil_base(int64_t p, int64_t inner, int n) 
   return o * (int64_t)n * inner + (p - o * inner);
 }
 
+// bulk prefetch of a contiguous global range into L2 (16-byte aligned address, size a multiple of 16)
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // chi(alpha) applied to the C-vector v at voxel vox: out_r = sum_s (a chi_rs + b delta_rs) v_s
 template <class R, int C, int CHI>
 __device__ __forceinline__ void apply_chi(const cpx<R>* __restrict__ chi, int64_t N, int64_t vox, const ChiCoef<R>& cc,
@@ -145,6 +150,44 @@ __device__ __forceinline__ void block_reduce_2(double x, double y, double* out2)
     if (lane == 0) {
       out2[0] = x;
       out2[1] = y;
+    }
+  }
+}
+
+// apply_chi at the neighbouring voxels vox and vox + 1 (vox even, N even), complex64: each stored chi entry of the
+// two voxels is one 16-byte load
+template <int C, int CHI>
+__device__ __forceinline__ void apply_chi2(const float2* __restrict__ chi, int64_t N, int64_t vox,
+                                           const ChiCoef<float>& cc, const float2* v0, const float2* v1, float2* o0,
+                                           float2* o1) {
+  constexpr int M = CHI == MMX_CHI_SCALAR ? 1 : (CHI == MMX_CHI_SYM6 ? 6 : 9);
+  float2 m0[M], m1[M];
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    const float4 w = *reinterpret_cast<const float4*>(chi + k * N + vox);
+    m0[k] = cc.a * make_float2(w.x, w.y);
+    m1[k] = cc.a * make_float2(w.z, w.w);
+  }
+  if constexpr (CHI == MMX_CHI_SCALAR) {
+    const float2 x0 = m0[0] + cc.b, x1 = m1[0] + cc.b;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      o0[c] = x0 * v0[c];
+      o1[c] = x1 * v1[c];
+    }
+  } else {
+    constexpr int K6[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      float2 a0 = cc.b * v0[r], a1 = cc.b * v1[r];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int k = CHI == MMX_CHI_SYM6 ? K6[r * 3 + s] : r * 3 + s;
+        a0 += m0[k] * v0[s];
+        a1 += m1[k] * v1[s];
+      }
+      o0[r] = a0;
+      o1[r] = a1;
     }
   }
 }

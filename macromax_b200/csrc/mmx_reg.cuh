@@ -460,10 +460,6 @@ __device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, unsi
                : "memory");
 }
 
-// bulk prefetch of a contiguous global range into L2 (16-byte aligned address, size a multiple of 16)
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 
 // in-place shared-memory stage for the contiguous layout
 template <int DIR, int N, int C, int PC_, int RAD, int L>

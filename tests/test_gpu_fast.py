@@ -52,6 +52,7 @@ def _cases():
         # anisotropic 3x3 eps with 192-sample strided axes (register-staged 8 x 8 x 3 pencils)
         'voronoi_192x64x64': lambda: _stacked_voronoi(0),
         'voronoi_64x192x64': lambda: _stacked_voronoi(1),
+        'voronoi_64x64x192': lambda: _stacked_voronoi(2),  # 192-sample rows: the 3x3-chi contiguous passes
         'mixed_3d': lambda: {**w.design_3d(n=64), 'shape': (64, 40, 64),
                              'epsilon': w.design_3d(n=64)['epsilon'][:, :40, :],
                              'source': w.design_3d(n=64)['source'][:, :, :40, :]},
@@ -102,7 +103,7 @@ def _solution_env(wl, env):
 
 
 @pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256', 'mixed_3d', 'voronoi_192x64x64',
-                                  'voronoi_64x192x64'])
+                                  'voronoi_64x192x64', 'voronoi_64x64x192'])
 def test_register_staged_matches_shared_staged(name):
     """k_reg_pass (strided passes, 16-pencil tiles, global<->register first/last stages) vs k_fast_pass."""
     wl = _cases()[name]()
