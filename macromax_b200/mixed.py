@@ -62,7 +62,8 @@ class MixedSolution:
                 m = pre.chi.shape[0] * pre.chi.shape[1]
                 chi = np.broadcast_to(pre.chi, (pre.chi.shape[0], pre.chi.shape[1], *grid.shape)).reshape(m, N)
                 # C order explicitly: a permittivity built as a strided view reshapes to a strided view too
-                self.chi64 = torch.from_numpy(np.ascontiguousarray(chi, dtype=np.complex128)).to(self.device)
+                self.chi64 = torch.from_numpy(np.require(np.ascontiguousarray(chi, dtype=np.complex128),
+                                                         requirements='W')).to(self.device)
             s0 = src.reshape(self.batch, self.ncomp, N) * (1.0j / pre.alpha.imag / pre.beta)
             # a 3x3 chi equal to its transpose in FP64 is kept as its six distinct entries, as the inner
             # iteration keeps its complex64 copy
@@ -75,21 +76,27 @@ class MixedSolution:
             self.src64 = torch.from_numpy(np.ascontiguousarray(s0, dtype=np.complex128)).to(self.device)
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
             self._norm = torch.zeros(1, dtype=torch.float64, device=self.device)
+            self._norms = torch.zeros(self.batch, dtype=torch.float64, device=self.device)
         self.outer_residues = []
         self.inner_iterations = []
 
-    def _xnorm(self, b):
-        nat.call('mmx_norm', self.plan64.handle, _ptr(self.x[b]), self.ncomp * self.inner.engine.N, nat.MMX_C128,
-                 _ptr(self._norm), _stream())
-        return float(self._norm.item())
+    def _xnorms(self) -> np.ndarray:
+        """FP64 norms of every right-hand side's x, read back once (the launches queue on one stream and share the
+        plan's scratch in order)."""
+        n = self.ncomp * self.inner.engine.N
+        for b in range(self.batch):
+            nat.call('mmx_norm', self.plan64.handle, _ptr(self.x[b]), n, nat.MMX_C128, _ptr(self._norms[b:b + 1]),
+                     _stream())
+        return self._norms.cpu().numpy()
 
     def solve(self, rtol: float = 1e-8, inner_rtol: float = 1e-4, inner_maxiter: int = 100000, max_outer: int = 30):
         eng = self.inner.engine
         done = np.zeros(self.batch, dtype=bool)
         for _ in range(max_outer):
             # every unconverged right-hand side is active for the defect and for one first correction step
-            eng.set_fields(torch.zeros((self.batch, self.ncomp, eng.N), dtype=eng.torch_dtype, device=self.device))
+            eng.fields.zero_()  # both buffers, in place (no batch-sized allocation)
             st = eng.read_state()
+            st['prev_norm'] = np.inf
             st['iteration'] = 0
             st['rtol'] = -1.0
             st['maxiter'] = 1
@@ -101,10 +108,9 @@ class MixedSolution:
             eng.iterate(1)  # first correction step: its update norm is ||d(x)||
             st = eng.read_state()
             res = np.full(self.batch, np.inf)
-            for b in range(self.batch):
-                xn = self._xnorm(b)
-                if xn > 0:
-                    res[b] = st['last_norm'][b] / xn
+            xn = self._xnorms()
+            pos = xn > 0
+            res[pos] = st['last_norm'][pos] / xn[pos]
             res[done] = 0.0
             self.outer_residues.append(res.copy())
             newly = (res < rtol) & ~done
@@ -125,10 +131,10 @@ class MixedSolution:
                     break
                 chunk = min(2 * chunk, 64)
             self.inner_iterations.append(st['iteration'].copy())
-            delta = eng.current(st)
-            for b in range(self.batch):
+            for b in range(self.batch):  # x += delta from the current buffer of each right-hand side (no gather)
                 if not done[b]:
-                    nat.call('mmx_accumulate', _ptr(self.x[b]), _ptr(delta[b]), self.ncomp * eng.N, _stream())
+                    nat.call('mmx_accumulate', _ptr(self.x[b]), _ptr(eng.fields[int(st['cur'][b]), b]),
+                             self.ncomp * eng.N, _stream())
         self.converged = done
         return self
 
