@@ -305,7 +305,7 @@ def run_secondary(args):
       - the standalone transform mmx_fftn (BackEnd.ft) of three 128^3 complex64 fields;
       - batched mixed precision (2D scalar slab, 512^2 grid, 256 plane-wave sources) to residue 1e-8, against the
         plain complex64 per-source loop (one Solution per source, to 1e-5: single precision cannot reach 1e-8),
-        measured on 4 sources and scaled to 256;
+        measured on 4 sources and scaled to 256; and the uneven batch 64 x 128^2 + 32 x 256^2 + 8 x 384^2 to 1e-8;
       - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve to 1e-6.
     """
     import torch
@@ -339,6 +339,27 @@ def run_secondary(args):
         its += sol.iteration
         sol._engine.close()
     plain_256 = seq / 4 * 256
+    # the uneven batch of the same material class: 64 x 128^2, 32 x 256^2 and 8 x 384^2 sources to 1e-8, all
+    # members' inner solves in one graph per chunk
+    from macromax_b200.mixed import MixedUnevenSolution
+    members = []
+    for n_, b_, seed_ in ((128, 64, 41), (256, 32, 42), (384, 8, 43)):
+        w_ = workloads.correlated_slab_2d(n=n_, nb_modes=b_, seed=seed_, slab_px=n_ // 4)
+        g_ = Grid(shape=w_['shape'], step=w_['step'])
+        members.append(MixedSolution(g_, w_['source'], w_['epsilon'], bound=Bound(g_, thickness=w_['bound_thickness']),
+                                     vacuum_wavelength=w_['wavelength']))
+    mu = MixedUnevenSolution(members)
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    mu.solve(rtol=1e-8)
+    torch.cuda.synchronize()
+    uneven_s = time.perf_counter() - a
+    work = sum(m.inner.engine.N * int(sum(np.sum(i) for i in m.inner_iterations)) for m in members)
+    out['uneven_mixed_slab2d_64x128^2_32x256^2_8x384^2'] = {
+        'time_to_1e-8_s': uneven_s, 'max_residue': float(max(m.residues.max() for m in members)),
+        'outer_steps': [len(m.outer_residues) for m in members],
+        'voxel_rhs_iterations_per_s': work / uneven_s}
+    mu.close()
     out['batched_mixed_slab2d_512x256'] = {
         'time_to_1e-8_s': mixed_s, 'max_residue': res, 'setup_s': t1 - t0, 'inner_iterations': inner,
         'plain_c64_loop_to_1e-5_s (4-source sample x 64)': plain_256, 'plain_iterations_per_source': its / 4,

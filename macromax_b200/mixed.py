@@ -89,53 +89,70 @@ class MixedSolution:
                      _stream())
         return self._norms.cpu().numpy()
 
+    # -- one outer step in phases (MixedUnevenSolution runs the inner solves of several grids together) ---------
+    def _outer_begin(self, rtol: float) -> bool:
+        """Defect and first correction step of every unconverged right-hand side; True when all have converged."""
+        eng = self.inner.engine
+        done = self._done
+        # every unconverged right-hand side is active for the defect and for one first correction step
+        eng.fields.zero_()  # both buffers, in place (no batch-sized allocation)
+        st = eng.read_state()
+        st['prev_norm'] = np.inf
+        st['iteration'] = 0
+        st['rtol'] = -1.0
+        st['maxiter'] = 1
+        st['active'] = (~done).astype(np.int32)
+        st['status'] = 0
+        eng.write_state(st)
+        nat.call('mmx_defect', self.plan64.handle, _ptr(self.x), _ptr(self.chi64), self.chi64_kind, _ptr(self.src64),
+                 _ptr(eng.state), _ptr(eng.sources), _stream())
+        eng.iterate(1)  # first correction step: its update norm is ||d(x)||
+        st = eng.read_state()
+        res = np.full(self.batch, np.inf)
+        xn = self._xnorms()
+        pos = xn > 0
+        res[pos] = st['last_norm'][pos] / xn[pos]
+        res[done] = 0.0
+        self.outer_residues.append(res.copy())
+        done |= (res < rtol) & ~done
+        if np.all(done):
+            return True
+        # the inner solves of the unconverged right-hand sides go on from here
+        st['iteration'] = 1
+        st['rtol'] = self._inner_rtol
+        st['maxiter'] = self._inner_maxiter
+        st['active'] = (~done).astype(np.int32)
+        eng.write_state(st)
+        return False
+
+    def _outer_end(self):
+        """x += delta for every right-hand side that was still correcting."""
+        eng = self.inner.engine
+        st = eng.read_state()
+        self.inner_iterations.append(st['iteration'].copy())
+        for b in range(self.batch):  # x += delta from the current buffer of each right-hand side (no gather)
+            if not self._done[b]:
+                nat.call('mmx_accumulate', _ptr(self.x[b]), _ptr(eng.fields[int(st['cur'][b]), b]),
+                         self.ncomp * eng.N, _stream())
+
+    def _start(self, inner_rtol: float, inner_maxiter: int):
+        self._done = np.zeros(self.batch, dtype=bool)
+        self._inner_rtol, self._inner_maxiter = inner_rtol, inner_maxiter
+
     def solve(self, rtol: float = 1e-8, inner_rtol: float = 1e-4, inner_maxiter: int = 100000, max_outer: int = 30):
         eng = self.inner.engine
-        done = np.zeros(self.batch, dtype=bool)
+        self._start(inner_rtol, inner_maxiter)
         for _ in range(max_outer):
-            # every unconverged right-hand side is active for the defect and for one first correction step
-            eng.fields.zero_()  # both buffers, in place (no batch-sized allocation)
-            st = eng.read_state()
-            st['prev_norm'] = np.inf
-            st['iteration'] = 0
-            st['rtol'] = -1.0
-            st['maxiter'] = 1
-            st['active'] = (~done).astype(np.int32)
-            st['status'] = 0
-            eng.write_state(st)
-            nat.call('mmx_defect', self.plan64.handle, _ptr(self.x), _ptr(self.chi64), self.chi64_kind, _ptr(self.src64),
-                     _ptr(eng.state), _ptr(eng.sources), _stream())
-            eng.iterate(1)  # first correction step: its update norm is ||d(x)||
-            st = eng.read_state()
-            res = np.full(self.batch, np.inf)
-            xn = self._xnorms()
-            pos = xn > 0
-            res[pos] = st['last_norm'][pos] / xn[pos]
-            res[done] = 0.0
-            self.outer_residues.append(res.copy())
-            newly = (res < rtol) & ~done
-            done |= newly
-            if np.all(done):
+            if self._outer_begin(rtol):
                 break
-            # finish the inner solves of the unconverged right-hand sides
-            st['iteration'] = 1
-            st['rtol'] = inner_rtol
-            st['maxiter'] = inner_maxiter
-            st['active'] = (~done).astype(np.int32)
-            eng.write_state(st)
             chunk = 8
             while True:
                 eng.iterate(chunk)
-                st = eng.read_state()
-                if not np.any(st['active']):
+                if not np.any(eng.read_state()['active']):
                     break
                 chunk = min(2 * chunk, 64)
-            self.inner_iterations.append(st['iteration'].copy())
-            for b in range(self.batch):  # x += delta from the current buffer of each right-hand side (no gather)
-                if not done[b]:
-                    nat.call('mmx_accumulate', _ptr(self.x[b]), _ptr(eng.fields[int(st['cur'][b]), b]),
-                             self.ncomp * eng.N, _stream())
-        self.converged = done
+            self._outer_end()
+        self.converged = self._done
         return self
 
     @property
@@ -158,3 +175,49 @@ class MixedSolution:
     def close(self):
         self.plan64.close()
         self.inner.close()
+
+
+class MixedUnevenSolution:
+    """
+    The mixed-precision solve for several batches on grids of different sizes (e.g. 64 x 128^2, 32 x 256^2 and
+    8 x 384^2 sources of one material class): each member keeps its own FP64 iterate, defect and complex64 inner
+    iteration (a MixedSolution), and in every outer step the inner solves of all members run together, one captured
+    CUDA graph per chunk of iterations with each member's passes as an independent branch (UnevenBatch).
+    """
+
+    def __init__(self, members):
+        from .batch import UnevenBatch
+        self.members = list(members)
+        self._uneven = UnevenBatch([m.inner for m in self.members])
+
+    def solve(self, rtol: float = 1e-8, inner_rtol: float = 1e-4, inner_maxiter: int = 100000, max_outer: int = 30):
+        for m in self.members:
+            m._start(inner_rtol, inner_maxiter)
+        for _ in range(max_outer):
+            finished = [m._outer_begin(rtol) if not np.all(m._done) else True for m in self.members]
+            if all(finished):
+                break
+            chunk = 8
+            while True:
+                self._uneven.iterate(chunk)
+                if not any(np.any(m.inner.engine.read_state()['active']) for m in self.members):
+                    break
+                chunk = min(2 * chunk, 64)
+            for m, f in zip(self.members, finished):
+                if not f:
+                    m._outer_end()
+        for m in self.members:
+            m.converged = m._done
+        return self
+
+    @property
+    def residues(self):
+        return [m.residues for m in self.members]
+
+    @property
+    def total_inner_iterations(self) -> int:
+        return max(m.total_inner_iterations for m in self.members)
+
+    def close(self):
+        for m in self.members:
+            m.close()

@@ -86,3 +86,33 @@ def test_mixed_anisotropic_strided_permittivity():
     ms.solve(rtol=1e-8)
     assert ms.converged.all() and ms.residues.max() < 1e-8
     ms.close()
+
+
+def _slab_member(n, nb_modes, seed):
+    from macromax_b200 import Bound, Grid, workloads
+    from macromax_b200.mixed import MixedSolution
+    wl = workloads.correlated_slab_2d(n=n, nb_modes=nb_modes, seed=seed, slab_px=n // 4)
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    return MixedSolution(grid, wl['source'], wl['epsilon'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                         vacuum_wavelength=wl['wavelength'])
+
+
+def test_mixed_uneven_batch_equals_separate_solves():
+    """Grids of three sizes (the uneven batch form, scaled down): the inner solves of all members run in one graph
+    per chunk; every member reaches 1e-8 with the same outer residues, inner iterations and FP64 field as its own
+    MixedSolution."""
+    from macromax_b200.mixed import MixedUnevenSolution
+    specs = [(64, 4, 11), (128, 3, 12), (96, 2, 13)]
+    joint = MixedUnevenSolution([_slab_member(*sp) for sp in specs])
+    joint.solve(rtol=1e-8)
+    for m, sp in zip(joint.members, specs):
+        alone = _slab_member(*sp).solve(rtol=1e-8)
+        assert m.converged.all() and m.residues.max() < 1e-8
+        assert len(m.outer_residues) == len(alone.outer_residues)
+        for r1, r2 in zip(m.outer_residues, alone.outer_residues):
+            np.testing.assert_allclose(r1, r2, rtol=1e-12)
+        for i1, i2 in zip(m.inner_iterations, alone.inner_iterations):
+            assert np.array_equal(i1, i2)
+        assert rel(m.E, alone.E) < 1e-13
+        alone.close()
+    joint.close()
