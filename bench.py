@@ -398,7 +398,24 @@ def run_secondary(args):
         'setup_s': b - a, 'time_to_1e-8_s': c - b, 'max_residue': float(ms.residues.max()),
         'inner_iterations': ms.total_inner_iterations, 'outer_steps': len(ms.outer_residues),
         'voxel_iterations_per_s': 192 ** 3 * ms.total_inner_iterations / (c - b)}
+    # error against an FP64 solution: the plain complex128 iteration on the device (the path pinned to the reference's
+    # iterates at 1e-10) run to residue 1e-11 (the FP64 numpy oracle would take hours at this size)
+    x64 = ms.E[0]
     ms.close()
+    sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'], source_distribution=wl['source'],
+                   bound=Bound(grid, thickness=wl['bound_thickness']), dtype=np.complex128)
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    sol.solve(None, rtol=1e-11, maxiter=20000)
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    ref = sol.E
+    out['anisotropic_voronoi3d_192_mixed']['error_vs_fp64_solution'] = float(
+        np.linalg.norm((x64 - ref).ravel()) / np.linalg.norm(ref.ravel()))
+    out['anisotropic_voronoi3d_192_mixed']['fp64_reference'] = {
+        'iterations': int(sol.iteration), 'residue': float(sol.residue), 'seconds': b - a}
+    sol._engine.close()
+    del x64, ref
     # magnetic medium: the reference test suite's negative-index plate (128^2, complex64) to residue 1e-3
     from macromax_b200 import LinearBound, solve
     wavelength, k0 = 500e-9, 2 * np.pi / 500e-9
