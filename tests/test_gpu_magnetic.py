@@ -100,3 +100,49 @@ def test_reference_negative_index_plate_known_answer():
     assert abs(np.linalg.norm(back.ravel()) - 0.0001864) < 1.5e-5  # numpy decimal=5, as in the reference test
     assert abs(np.linalg.norm(front.ravel()) - 0.0002582) < 1.5e-5
     assert E.dtype == np.complex64
+
+
+def test_magnetic_building_blocks_match_numpy():
+    """The per-op entry points behind BackEnd.curl and the magnetic chi_op (mmx_curl_ft, mmx_green_ft, mmx_chi_mix,
+    mmx_axpby) against numpy restatements (the oracle's curl_ft and longitudinal projection), complex128."""
+    import ctypes
+    import torch
+    from macromax_b200 import _native as nat
+    from oracle import mmoracle as mo
+    shape, step, k0 = (6, 10, 8), 0.3, 1.7
+    ndim, N = len(shape), int(np.prod(shape))
+    rng = np.random.default_rng(9)
+    cplx = lambda *s: rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    ks = mo.k_vectors(shape, (step,) * ndim, k0)
+    plan = nat.Plan(shape, 1, 1, nat.MMX_C128)
+    plan.set_kvectors([np.asarray(k, dtype=np.float64).ravel() for k in ks])
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex128)).cuda()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    F = cplx(3, *shape)
+    Ft, out = dev(F.reshape(3, N)), dev(np.zeros((3, N)))
+    nat.call('mmx_curl_ft', plan.handle, nat.device_ptr(Ft), nat.device_ptr(out), s)
+    ref = mo.curl_ft(F, ks)
+    assert rel(out.cpu().numpy().reshape(ref.shape), ref) < 1e-14
+    alpha = 1.3 + 0.4j
+    nat.call('mmx_green_ft', plan.handle, nat.device_ptr(Ft), alpha.real, alpha.imag, s)
+    pl = mo.longitudinal_projection_ft(F[:, None], ks, ndim)[:, 0]
+    g = -1j * alpha.imag / (mo.k2_field(ks) - alpha)
+    ref = g * (F - pl) + (1j * alpha.imag / alpha) * pl
+    assert rel(Ft.cpu().numpy().reshape(ref.shape), ref) < 1e-13
+    x, d = cplx(3, N), cplx(3, N)
+    blocks = [cplx(3, 3, N) for _ in range(4)]  # EE, EH, HE, HH
+    coef = [0.8 + 0.1j, 0.2 - 0.3j, 1.1 + 0.0j, 0.9 - 0.2j, 0.7 + 0.4j]
+    u, w = dev(np.zeros((3, N))), dev(np.zeros((3, N)))
+    bt = [dev(bk.reshape(9, N)) for bk in blocks]
+    cvals = (ctypes.c_double * 10)(*[v for c in coef for v in (c.real, c.imag)])
+    nat.call('mmx_chi_mix', nat.device_ptr(dev(x)), nat.device_ptr(dev(d)), *[nat.device_ptr(t) for t in bt], cvals,
+             nat.device_ptr(u), nat.device_ptr(w), N, nat.MMX_C128, s)
+    mv = lambda m, v: np.einsum('rsn,sn->rn', m, v)
+    ref_u = coef[0] * mv(blocks[0], x) + coef[1] * x + coef[3] * mv(blocks[2], d)
+    ref_w = coef[2] * mv(blocks[1], x) + coef[4] * mv(blocks[3], d)
+    assert rel(u.cpu().numpy(), ref_u) < 1e-14 and rel(w.cpu().numpy(), ref_w) < 1e-14
+    o = dev(np.zeros((3, N)))
+    nat.call('mmx_axpby', nat.device_ptr(o), nat.device_ptr(dev(x)), nat.device_ptr(dev(d)), 0.5, -1.0, 2.0, 0.25,
+             3 * N, nat.MMX_C128, s)
+    assert rel(o.cpu().numpy(), (0.5 - 1j) * x + (2 + 0.25j) * d) < 1e-15
+    plan.close()
