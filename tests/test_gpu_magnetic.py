@@ -135,14 +135,15 @@ def test_magnetic_building_blocks_match_numpy():
     u, w = dev(np.zeros((3, N))), dev(np.zeros((3, N)))
     bt = [dev(bk.reshape(9, N)) for bk in blocks]
     cvals = (ctypes.c_double * 10)(*[v for c in coef for v in (c.real, c.imag)])
-    nat.call('mmx_chi_mix', nat.device_ptr(dev(x)), nat.device_ptr(dev(d)), *[nat.device_ptr(t) for t in bt], cvals,
+    xt, dt = dev(x), dev(d)  # kept alive: a temporary's memory would be reused by the next allocation
+    nat.call('mmx_chi_mix', nat.device_ptr(xt), nat.device_ptr(dt), *[nat.device_ptr(t) for t in bt], cvals,
              nat.device_ptr(u), nat.device_ptr(w), N, nat.MMX_C128, s)
     mv = lambda m, v: np.einsum('rsn,sn->rn', m, v)
     ref_u = coef[0] * mv(blocks[0], x) + coef[1] * x + coef[3] * mv(blocks[2], d)
     ref_w = coef[2] * mv(blocks[1], x) + coef[4] * mv(blocks[3], d)
     assert rel(u.cpu().numpy(), ref_u) < 1e-14 and rel(w.cpu().numpy(), ref_w) < 1e-14
     o = dev(np.zeros((3, N)))
-    nat.call('mmx_axpby', nat.device_ptr(o), nat.device_ptr(dev(x)), nat.device_ptr(dev(d)), 0.5, -1.0, 2.0, 0.25,
+    nat.call('mmx_axpby', nat.device_ptr(o), nat.device_ptr(xt), nat.device_ptr(dt), 0.5, -1.0, 2.0, 0.25,
              3 * N, nat.MMX_C128, s)
     assert rel(o.cpu().numpy(), (0.5 - 1j) * x + (2 + 0.25j) * d) < 1e-15
     plan.close()
