@@ -16,7 +16,6 @@ from __future__ import annotations
 from math import inf
 
 import numpy as np
-import scipy.constants as const
 import torch
 
 from . import _native as nat

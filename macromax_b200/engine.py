@@ -8,7 +8,6 @@ only edits the small state array between calls (reset of the update norm, stop r
 """
 from __future__ import annotations
 
-import math
 
 import numpy as np
 import torch

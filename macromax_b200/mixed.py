@@ -75,7 +75,6 @@ class MixedSolution:
                 self.chi64_kind = nat.MMX_CHI_SYM6
             self.src64 = torch.from_numpy(np.ascontiguousarray(s0, dtype=np.complex128)).to(self.device)
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
-            self._norm = torch.zeros(1, dtype=torch.float64, device=self.device)
             self._norms = torch.zeros(self.batch, dtype=torch.float64, device=self.device)
         self.outer_residues = []
         self.inner_iterations = []
