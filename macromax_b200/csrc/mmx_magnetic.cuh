@@ -4,7 +4,7 @@
 // spectral curl i k x (backend/__init__.py:472-509; k of the k0-scaled grid).  It is applied twice per iteration,
 // so an iteration costs four curls (FFT pairs) plus the Green function's FFT pair; the host composes it from the
 // batched FFT (mmx_fftn) and the pointwise kernels below:
-//   k_curl_ft:   F -> i k x F for a 3-component spectrum [3][N]
+//   k_curl_ft:   F -> i k x F for a 3-component spectrum [3][N] (optionally add + i k x (F - sub))
 //   k_green_ft:  the dyadic Green multiply g (F - P_L F) + (i a_i / a) P_L F (reference DC and missing-axis rules)
 //   k_chi_mix:   u = chi_EE(alpha) x + chi_HE(alpha) d, w = chi_EH(alpha) x + chi_HH(alpha) d per voxel, with the four
 //                3x3 blocks stored once at alpha0 and rescaled on the fly (solver.py:514-528)
@@ -30,22 +30,35 @@ __device__ __forceinline__ void k_of_voxel(const KGrid& g, const R* const* kv, i
   }
 }
 
+// out = add + i k x (F - sub); add and sub may be null (then 0); add may be out itself (each voxel is read before
+// it is written, by the same thread)
 template <class R>
-__global__ void k_curl_ft(const cpx<R>* __restrict__ F, cpx<R>* __restrict__ out, KGrid g, const R* kv0,
-                          const R* kv1, const R* kv2) {
+__global__ void k_curl_ft(const cpx<R>* __restrict__ F, cpx<R>* out, KGrid g, const R* kv0, const R* kv1,
+                          const R* kv2, const cpx<R>* add = nullptr, const cpx<R>* __restrict__ sub = nullptr) {
   const R* kv[3] = {kv0, kv1, kv2};
   const int64_t N = g.N;
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < N; v += (int64_t)gridDim.x * blockDim.x) {
     R k[3];
     k_of_voxel<R>(g, kv, v, k);
-    const cpx<R> f0 = F[v], f1 = F[N + v], f2 = F[2 * N + v];
+    cpx<R> f0 = F[v], f1 = F[N + v], f2 = F[2 * N + v];
+    if (sub) {
+      f0 -= sub[v];
+      f1 -= sub[N + v];
+      f2 -= sub[2 * N + v];
+    }
     // (k x F)_d = k_{d+1} F_{d-1} - k_{d-1} F_{d+1}; axes beyond the grid have k = 0
     const cpx<R> c0 = k[1] * f2 - k[2] * f1;
     const cpx<R> c1 = k[2] * f0 - k[0] * f2;
     const cpx<R> c2 = k[0] * f1 - k[1] * f0;
-    out[v] = mul_i(c0, 1);
-    out[N + v] = mul_i(c1, 1);
-    out[2 * N + v] = mul_i(c2, 1);
+    if (add) {
+      out[v] = add[v] + mul_i(c0, 1);
+      out[N + v] = add[N + v] + mul_i(c1, 1);
+      out[2 * N + v] = add[2 * N + v] + mul_i(c2, 1);
+    } else {
+      out[v] = mul_i(c0, 1);
+      out[N + v] = mul_i(c1, 1);
+      out[2 * N + v] = mul_i(c2, 1);
+    }
   }
 }
 
@@ -137,13 +150,13 @@ __global__ void k_axpby(cpx<R>* __restrict__ out, const cpx<R>* __restrict__ x, 
 // decision), so that its accepted update is still applied when the stop rule then ends the solve.
 // ---------------------------------------------------------------------------------------------------------------
 
-// out = u + dx + (alpha0_i / alpha_i) s   (chi E + s'(alpha), the Green function's input)
+// out = u + (alpha0_i / alpha_i) s   (the spatial part of chi E + s'(alpha) whose curl term is added in k-space)
 template <class R>
-__global__ void k_mag_sum_src(cpx<R>* __restrict__ out, const cpx<R>* __restrict__ u, const cpx<R>* __restrict__ dx,
-                              const cpx<R>* __restrict__ src, const mmx_rhs_state* st, int64_t n) {
+__global__ void k_mag_usrc(cpx<R>* __restrict__ out, const cpx<R>* __restrict__ u, const cpx<R>* __restrict__ src,
+                           const mmx_rhs_state* st, int64_t n) {
   const R f = (R)(st->alpha0_im / st->alpha_im);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = u[i] + dx[i] + f * src[i];
+    out[i] = u[i] + f * src[i];
 }
 
 // d = u + dx, with per-block FP64 partial sums of |d|^2, |E + d|^2 and |E|^2 (partials [gridDim.x][3])
