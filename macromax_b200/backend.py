@@ -293,7 +293,8 @@ class BackEndB200:
         return self._k2
 
     def longitudinal_projection_ft(self, F):
-        """backend/__init__.py:606-649 (DC passed through, components >= ndim zero)."""
+        """backend/__init__.py:606-649 (DC passed through, components >= ndim zero); a per-op tensor expression (the
+        fused iteration applies the projection inside its axis-0 pass)."""
         F = self.astype(F)
         nd = self._grid.ndim
         proj = F[0, 0] * self.k[0]
@@ -315,9 +316,14 @@ class BackEndB200:
         return F - self.longitudinal_projection_ft(F)
 
     def curl_ft(self, F):
-        """backend/__init__.py:483-509."""
+        """backend/__init__.py:483-509: i k x F.  A 3-component field of this grid goes through mmx_curl_ft."""
         F = self.astype(F)
         n = self._nb_rows
+        if n == 3 and F.shape[0] == 3 and F.numel() == 3 * self._grid.size:
+            Fc = F.contiguous()
+            out = torch.empty_like(Fc)
+            nat.call('mmx_curl_ft', self._plan.handle, _ptr(Fc), _ptr(out), _stream())
+            return out
         out = torch.zeros((n, *F.shape[1:]), dtype=self._tdtype, device=self._device)
         for d in range(n):
             o = (d + np.array([-1, 1])) % n
