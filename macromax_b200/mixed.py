@@ -46,8 +46,11 @@ class MixedSolution:
         src = np.asarray(sources)
         if src.ndim == grid.ndim + 1:
             src = src[np.newaxis]
-        self.inner = BatchSolution(grid, np.zeros_like(src), None, bound=bound, wavenumber=self.wavenumber,
-                                   dtype=np.complex64, device=device, preconditioner=pre)
+        # the inner iteration's sources are the defects, written on the device: start them at zero there
+        dev0 = torch.device(device if device is not None else 'cuda')
+        self.inner = BatchSolution(grid, torch.zeros(src.shape, dtype=torch.complex64, device=dev0), None,
+                                   bound=bound, wavenumber=self.wavenumber, dtype=np.complex64, device=device,
+                                   preconditioner=pre)
         self.pre = pre
         self.batch, self.ncomp = self.inner.batch, self.inner.ncomp
         eng = self.inner.engine
@@ -64,7 +67,6 @@ class MixedSolution:
                 # C order explicitly: a permittivity built as a strided view reshapes to a strided view too
                 self.chi64 = torch.from_numpy(np.require(np.ascontiguousarray(chi, dtype=np.complex128),
                                                          requirements='W')).to(self.device)
-            s0 = src.reshape(self.batch, self.ncomp, N) * (1.0j / pre.alpha.imag / pre.beta)
             # a 3x3 chi equal to its transpose in FP64 is kept as its six distinct entries, as the inner
             # iteration keeps its complex64 copy
             self.chi64_kind = eng.chi_kind if eng.chi_kind == nat.MMX_CHI_SCALAR else nat.MMX_CHI_MAT3
@@ -73,7 +75,11 @@ class MixedSolution:
                     and torch.equal(c[5], c[7]):
                 self.chi64 = c[list(nat.SYM6_ROWS)].contiguous()
                 self.chi64_kind = nat.MMX_CHI_SYM6
-            self.src64 = torch.from_numpy(np.ascontiguousarray(s0, dtype=np.complex128)).to(self.device)
+            # s'0 = i s / (alpha_i beta) in FP64, scaled on the device (one upload of the sources, no host copy when
+            # they are already contiguous complex128)
+            s_host = np.require(np.ascontiguousarray(src, dtype=np.complex128), requirements='W')
+            self.src64 = torch.from_numpy(s_host).to(self.device).reshape(self.batch, self.ncomp, N)
+            self.src64 *= 1.0j / pre.alpha.imag / pre.beta
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
             self._norms = torch.zeros(self.batch, dtype=torch.float64, device=self.device)
         self.outer_residues = []
