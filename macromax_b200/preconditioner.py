@@ -199,6 +199,11 @@ def prepare(eps_field: np.ndarray, thickness: np.ndarray, wavenumber: float, eps
     if device_setup and not _is_scalar_field(eps_field):
         dev = DeviceSetup(eps_field, device)
         gain, loss = dev.gain_loss(eps_dtype)
+    elif _is_scalar_field(eps_field):
+        # for a scalar permittivity -0.5i (eps - conj(eps)) is Im(eps) exactly, so has_gain's test is on Im(eps)
+        im = np.asarray(eps_field[0, 0]).imag
+        thr = math.sqrt(eps_dtype)
+        gain, loss = bool(np.any(im < -thr)), bool(np.any(im > thr))
     else:
         gain = has_gain(eps_field, eps_dtype)
         loss = has_gain(-eps_field, eps_dtype)

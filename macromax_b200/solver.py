@@ -267,6 +267,12 @@ class Solution:
         if E is None:
             return
         E = np.asarray(E)
+        if E.ndim == 0:  # a constant field is filled on the device
+            import torch
+            eng = self._engine
+            self._engine.set_fields(torch.full((1, eng.ncomp, eng.N), complex(E) * self._wavenumber ** 2,
+                                               dtype=eng.torch_dtype, device=eng.device))
+            return
         full = np.broadcast_to(self._to_matrix_field(E), (self._nb_pol, 1, *self._grid.shape))[:, 0]
         self._engine.set_fields(full * (self._wavenumber ** 2))
 
