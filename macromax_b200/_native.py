@@ -16,13 +16,16 @@ from . import build as _build
 
 LIB_PATH = _build.LIB_PATH
 
-MMX_OK = 0
 MMX_C64 = 0
 MMX_C128 = 1
 MMX_CHI_SCALAR = 1
 MMX_CHI_MAT3 = 9
 MMX_CHI_SYM6 = 6
 SYM6_ROWS = (0, 1, 2, 4, 5, 8)  # xx, xy, xz, yy, yz, zz of a row-major 3x3
+MMX_OK = 0
+MMX_ERR_ARG = -1
+MMX_ERR_CUDA = -2
+MMX_ERR_UNSUPPORTED = -3
 MMX_STATUS_OK = 0
 MMX_STATUS_ZERODIV = 1
 MMX_STATUS_TIMEOUT = 2

@@ -186,10 +186,13 @@ class IterationEngine:
         nat.call('mmx_iterate_graph_prepare', self.plan.handle, _ptr(self.fields[0]), _ptr(self.fields[1]),
                  _ptr(self.chi), self.chi_kind, _ptr(self.sources), _ptr(self.state), int(niter))
 
-    def run(self, rtol: float, maxiter: float, chunk: int = 8, max_chunk: int = 64) -> np.ndarray:
-        """Iterate every active RHS until its stop rule (iteration < maxiter and residue > rtol) fails."""
+    def run(self, rtol: float, maxiter: float, chunk: int = 8, max_chunk: int = 64,
+            reset_iteration: bool = True) -> np.ndarray:
+        """Iterate every active RHS until its stop rule (iteration < maxiter and residue > rtol) fails; the iteration
+        count starts from 0, or goes on from its current value (reset_iteration=False, as Solution.solve does)."""
         st = self.read_state()
-        st['iteration'] = 0
+        if reset_iteration:
+            st['iteration'] = 0
         st['rtol'] = rtol
         st['maxiter'] = maxiter
         st['active'] = 1

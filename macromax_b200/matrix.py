@@ -283,6 +283,7 @@ class ScatteringMatrix:
         sol = self._solution
         sol.source_distribution = source
         sol.E = 0
+        sol.iteration = 0  # every column gets its own iteration budget (the batched columns do the same)
         sol.solve(self._callback if self._callback is not None else _default_callback)
         if out is None:
             return sol.E

@@ -321,15 +321,17 @@ class Solution:
 
     # -- iteration --------------------------------------------------------------------------------------------------
     def __iter__(self):
-        """solver.py:1049-1098: every next() runs one fused iteration on the device."""
+        """solver.py:1049-1098: every next() runs one fused iteration on the device; the iteration count goes on
+        from its current value, and a zero update norm after a zero one raises ZeroDivisionError (solver.py:1079)."""
         st = self._engine.read_state()
-        st['iteration'] = 0
         st['rtol'] = -1.0
         st['maxiter'] = np.inf
         st['active'] = 1
+        st['status'] = 0
         self._engine.write_state(st)
         while True:
             self._engine.iterate(1)
+            self._check_status(self._state)
             yield self
 
     def solve(self, callback: Callable[['Solution'], bool] | None = _default_callback, rtol: float = 0,
@@ -338,11 +340,10 @@ class Solution:
         if callback is None or callback is _default_callback:
             if callback is _default_callback:
                 rtol, maxiter = 1e-4, 1e4
-            st = self._engine.run(float(rtol), float(maxiter))
+            st = self._engine.run(float(rtol), float(maxiter), reset_iteration=False)
             self._check_status(st[0])
             return self
         for sol in self:
-            self._check_status(self._state)
             if not callback(sol):
                 break
         return self

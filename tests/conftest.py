@@ -23,6 +23,11 @@ def gpu_available() -> bool:
 
 
 def pytest_collection_modifyitems(config, items):
+    # a test that loops on the host without end fails after 5 minutes instead of holding the run (pytest-timeout)
+    if config.pluginmanager.hasplugin('timeout'):
+        for item in items:
+            if item.get_closest_marker('timeout') is None:
+                item.add_marker(pytest.mark.timeout(300))
     if gpu_available():
         return
     skip = pytest.mark.skip(reason='no CUDA device in this environment')
