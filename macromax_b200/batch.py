@@ -106,7 +106,9 @@ class BatchSolution:
         E = np.broadcast_to(np.asarray(E), (self.batch, self.ncomp, *self.grid.shape))
         self.engine.set_fields(E * self.wavenumber ** 2)
 
-    def solve(self, rtol: float = 1e-6, maxiter=inf) -> 'BatchSolution':
+    def solve(self, rtol: float = 1e-6, maxiter=1e4) -> 'BatchSolution':
+        """Iterate every source until its residue is below rtol or it has made maxiter iterations (by default the
+        reference's default cap, solver.py:81-83: complex64 alone may never reach a small rtol)."""
         st = self.engine.run(float(rtol), float(maxiter))
         if np.any(st['status'] == nat.MMX_STATUS_ZERODIV):
             raise ZeroDivisionError('float division by zero (update norm after a zero update norm)')
@@ -185,7 +187,7 @@ class UnevenBatch:
         s = torch.cuda.current_stream().cuda_stream
         nat.call('mmx_iterate_multi', *self._args, int(niter), ctypes.c_void_p(s) if s else None)
 
-    def solve(self, rtol: float = 1e-6, maxiter=inf, chunk: int = 8, max_chunk: int = 64) -> 'UnevenBatch':
+    def solve(self, rtol: float = 1e-6, maxiter=1e4, chunk: int = 8, max_chunk: int = 64) -> 'UnevenBatch':
         for m in self.members:
             st = m.engine.read_state()
             st['iteration'] = 0
