@@ -82,6 +82,7 @@ struct PassCfg {
   int plane = 0; // 1: plane pass over the two inner axes of a 3D grid (k_plane_pass), 2-CTA clusters
   int epro = 0;  // 1: epilogue fused with the next iteration's speculative prologue (k_regc_epro)
   int repair = 0;  // 1: prologue again for rejected right-hand sides (k_regc_repair)
+  int regc_aniso = 0;  // 1: register-staged contiguous pass for a 3x3 chi (k_regc_aniso_pass), rc_tiles / rc_smem
   int64_t rc_tiles = 0;
   size_t rc_smem = 0;
 };
@@ -345,6 +346,25 @@ int launch_regc(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   }
 }
 
+template <int OPS, int N, int CHI>
+int launch_regc_aniso(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  constexpr int PCK = RegCDefault<3, N>::PC;
+  auto kern = k_regc_aniso_pass<OPS, N, PCK, CHI>;
+  static int configured_mask = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(configured_mask & (1 << dev))) {
+    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
+    configured_mask |= (1 << dev);
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  dim3 grid((unsigned)pc.rc_tiles, (unsigned)batch);
+  MMX_CUDA(launch_pass(kern, grid, dim3(RegC<3, N, PCK>::THREADS), pc.rc_smem, s, a));
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
 int sm_count() {
   static int n = 0;
   if (!n) {
@@ -482,6 +502,15 @@ int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_
       default: break;
     }
   }
+  if constexpr (CHI != MMX_CHI_SCALAR && C == 3 && N == 192) {
+    if (pc.regc_aniso) {
+      switch (pc.ops) {
+        case OP_PRO | OP_FWD: return launch_regc_aniso<OP_PRO | OP_FWD, N, CHI>(pc, a, batch, s);
+        case OP_INV | OP_EPI: return launch_regc_aniso<OP_INV | OP_EPI, N, CHI>(pc, a, batch, s);
+        default: break;
+      }
+    }
+  }
   if (pc.regc && CHI == MMX_CHI_SCALAR) {
     switch (pc.ops) {
       case OP_PRO | OP_FWD: return launch_regc<C, OP_PRO | OP_FWD, N>(pc, a, batch, s);
@@ -593,6 +622,15 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
           pc.regc = 1;
           pc.rc_tiles = outer / pcr;
           pc.rc_smem = ((size_t)p->ncomp * pcr * (n + n / 16) + n) * sizeof(float2);
+        }
+      }
+      if (contig_op && inner == 1 && n == 192 && p->ncomp == 3 && !p->no_reg) {
+        // a 3x3 chi on 192-sample rows (the anisotropic 192^3 grids); an isotropic chi keeps k_fast_pass here
+        constexpr int pca = RegCDefault<3, 192>::PC;
+        if (outer % pca == 0) {
+          pc.regc_aniso = 1;
+          pc.rc_tiles = outer / pca;
+          pc.rc_smem = ((size_t)3 * pca * (n + n / 16) + n) * sizeof(float2);
         }
       }
       if (strided_op && inner % kRegP == 0 && reg_strided_length(n, p->ncomp) && !p->no_reg) {

@@ -706,6 +706,170 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
 }
 
 // ---------------------------------------------------------------------------------------------------------------
+// Contiguous prologue / epilogue passes for a 3x3 chi (MMX_CHI_SYM6 or MMX_CHI_MAT3) on a 3-component field, for
+// rows whose first radix stage has exactly C TPP butterflies (192 = 8 x 8 x 3: 24 per row).  The matrix couples
+// the components at each voxel, so the stages that apply it give one thread all three components of a butterfly
+// slot: the prologue's first stage forms (chi E + s')_c for c = 0..2 at the slot's samples (each E, s' and chi word
+// loaded once) and runs three butterflies; the epilogue reads the inverse transform of all three components back
+// from shared memory and forms d = chi (T - E) per sample.  The middle and the other outer stage keep the
+// per-component layout of k_regc_pass.
+// ---------------------------------------------------------------------------------------------------------------
+template <int CHI> __device__ __forceinline__ int chi_entry(int r, int s) {
+  if constexpr (CHI == MMX_CHI_SYM6) {
+    constexpr int K6[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    return K6[r * 3 + s];
+  } else {
+    return r * 3 + s;
+  }
+}
+
+template <int OPS, int N, int PC_, int CHI>
+__global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_pass(IterArgs<float> a) {
+  constexpr int C = 3;
+  using G = RegC<C, N, PC_>;
+  using PA = RegPlanArgs<typename RegPlan<N>::type>;
+  constexpr int TPP = G::TPP, PC = G::PC, THREADS = G::THREADS;
+  constexpr int M = CHI == MMX_CHI_SYM6 ? 6 : 9;
+  constexpr int RAD = PA::R_first;
+  constexpr int T1 = N / RAD;  // first-stage butterflies per row
+  static_assert(T1 == C * TPP, "one (row, butterfly slot) item per thread");
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * PC * G::PITCH;
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  const int64_t N3 = a.N;
+  const int64_t row0 = (int64_t)blockIdx.x * PC * N;
+  const unsigned chunk = (unsigned)(PC * N * sizeof(float2));
+  if (threadIdx.x < M) prefetch_l2(a.chi + (int64_t)threadIdx.x * N3 + row0, chunk);  // chi: no kernel writes it
+  if constexpr ((OPS & OP_PRO) != 0) {
+    if (threadIdx.x >= 32 && threadIdx.x < 32 + C)
+      prefetch_l2(a.src + ((int64_t)b * C + threadIdx.x - 32) * N3 + row0, chunk);
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
+  const ChiCoef<float> cc = chi_coef<float>(st);
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;          // per-component layout (FFT stages)
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int irow = tid / T1;         // all-component layout (chi stages): row and butterfly slot
+  const int islot = tid % T1;
+  const int64_t fbase = (int64_t)b * C * N3;
+  const int cur = st->cur;
+  const float2* __restrict__ Ecur = cur ? a.E1 : a.E0;
+  float2* __restrict__ Eoth = cur ? a.E0 : a.E1;
+  if (tid >= 64 && tid < 64 + C) prefetch_l2(Ecur + fbase + (int64_t)(tid - 64) * N3 + row0, chunk);
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  __syncthreads();
+  const int64_t ibase = ((int64_t)blockIdx.x * PC + irow) * N;  // voxel of sample 0 of the item's row
+  const float2* __restrict__ eI = Ecur + fbase + ibase;          // component r at eI[r N3 + sample]
+  const float2* __restrict__ xI = a.chi + ibase;                 // entry k at xI[k N3 + sample]
+  constexpr int RL = PA::R_last;
+  constexpr int TL = N / RL;
+  constexpr int NBL = TL / TPP;
+
+  if constexpr (OPS == (OP_PRO | OP_FWD)) {
+    const float2* __restrict__ sI = a.src + fbase + ibase;
+    float2 u[C][RAD];
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) {
+      const int s_ = islot + q * T1;
+      float2 e[C], m[M];
+#pragma unroll
+      for (int r = 0; r < C; ++r) e[r] = eI[r * N3 + s_];
+#pragma unroll
+      for (int k = 0; k < M; ++k) m[k] = cc.a * xI[k * N3 + s_];
+#pragma unroll
+      for (int r = 0; r < C; ++r) {
+        float2 acc = cc.b * e[r] + cc.s * sI[r * N3 + s_];
+#pragma unroll
+        for (int s2 = 0; s2 < C; ++s2) acc += m[chi_entry<CHI>(r, s2)] * e[s2];
+        u[r][q] = acc;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      bfly<float, RAD, -1>(u[r], smtw, N);
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) sm[G::idx(r, irow, islot * RAD + q)] = u[r][q];
+    }
+    __syncthreads();
+    PA::template mid<-1, N, C, PC>(sm, smtw);
+    float2* __restrict__ tO = a.T + fbase + c * N3 + ((int64_t)blockIdx.x * PC + row) * N;
+#pragma unroll 1
+    for (int mm = 0; mm < NBL; ++mm) {
+      const int i = ii + mm * TPP;
+      float2 v[RL];
+#pragma unroll
+      for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+      for (int q = 1; q < RL; ++q) v[q] = v[q] * smtw[q * i];
+      bfly<float, RL, -1>(v, smtw, N);
+#pragma unroll
+      for (int q = 0; q < RL; ++q) tO[i + q * TL] = v[q];
+    }
+  } else {
+    // INV | EPI: the inverse transform in the per-component layout, its outputs back in shared memory at their
+    // natural positions, then the epilogue in the all-component layout
+    constexpr int NBT = T1 / TPP;
+    const float2* __restrict__ tI = a.T + fbase + c * N3 + ((int64_t)blockIdx.x * PC + row) * N;
+#pragma unroll 1
+    for (int mm = 0; mm < NBT; ++mm) {
+      const int i = ii + mm * TPP;
+      float2 v[RAD];
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) v[q] = tI[i + q * T1];
+      bfly<float, RAD, +1>(v, smtw, N);
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = v[q];
+    }
+    __syncthreads();
+    PA::template mid<+1, N, C, PC>(sm, smtw);
+#pragma unroll 1
+    for (int mm = 0; mm < NBL; ++mm) {
+      const int i = ii + mm * TPP;
+      float2 v[RL];
+#pragma unroll
+      for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+      for (int q = 1; q < RL; ++q) v[q] = v[q] * conjc(smtw[q * i]);
+      bfly<float, RL, +1>(v, smtw, N);
+#pragma unroll
+      for (int q = 0; q < RL; ++q) sm[G::idx(c, row, i + q * TL)] = v[q];  // the positions this thread read
+    }
+    __syncthreads();
+    double dd2 = 0.0, en2 = 0.0;
+    float2* __restrict__ eO = Eoth + fbase + ibase;
+#pragma unroll 2
+    for (int q = 0; q < N / T1; ++q) {
+      const int s_ = islot + q * T1;
+      float2 e[C], diff[C], m[M];
+#pragma unroll
+      for (int r = 0; r < C; ++r) {
+        e[r] = eI[r * N3 + s_];
+        diff[r] = sm[G::idx(r, irow, s_)] - e[r];
+      }
+#pragma unroll
+      for (int k = 0; k < M; ++k) m[k] = cc.a * xI[k * N3 + s_];
+#pragma unroll
+      for (int r = 0; r < C; ++r) {
+        float2 d = cc.b * diff[r];
+#pragma unroll
+        for (int s2 = 0; s2 < C; ++s2) d += m[chi_entry<CHI>(r, s2)] * diff[s2];
+        const float2 en = e[r] + d;
+        eO[r * N3 + s_] = en;
+        dd2 += norm2d(d);
+        en2 += norm2d(en);
+      }
+    }
+    finish_pass_norms(a, b, dd2, en2);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
 // Persistent, double-buffered variants of the contiguous prologue / epilogue passes.
 //
 // Each CTA walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ... of all right-hand sides.  The inputs of a tile
