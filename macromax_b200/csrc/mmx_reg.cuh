@@ -22,6 +22,12 @@ template <> struct RegPlan<192> { using type = RegPlanList<8, 8, 3>; static cons
 
 constexpr int kRegP = 16;
 
+// Radix order of the axis-0 pass with the fused Green stage (3-component fields): that stage holds one (pencil,
+// butterfly) item per thread, P x N / R of them, so its radix R (the last forward one) must be the largest; for 192
+// the radix-3 stage goes first (P x 192 / 8 = 384 items, the block size).
+template <int N> struct GreenPlan { using type = typename RegPlan<N>::type; };
+template <> struct GreenPlan<192> { using type = RegPlanList<3, 8, 8>; };
+
 template <int C, int N> struct RegThreads {
   static constexpr int value = C * kRegP * RegPlan<N>::TPP;
 };
@@ -307,7 +313,7 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
       green_fused_scalar<N, RL>(sm, smtw, sk0, sk1, sk2, ar, ai, ai * ai * a.inv_total, -ai * a.inv_total);
       RChain<+1, N, 1, false, true, RL, typename PlanReverse<Init>::type>::run(sm, smtw, tile, tile, inner, a.N);
       return;
-    } else if constexpr (C == 3 && N == 128) {
+    } else if constexpr (C == 3 && (N == 128 || N == 192)) {
       // vector field: the same fused schedule with the dyadic Green multiply (all three components per item)
       if (tid < P) {
         const int64_t p = in0 + tid;
@@ -324,8 +330,9 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArg
         sk2[tid] = k2;
       }
       for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
-      using Init = typename PlanInit<Plan>::type;
-      constexpr int RL = PlanLast<Plan>::value;
+      using GPlan = typename GreenPlan<N>::type;
+      using Init = typename PlanInit<GPlan>::type;
+      constexpr int RL = PlanLast<GPlan>::value;
       RChain<-1, N, 3, true, false, 1, Init>::run(sm, smtw, tile, tile, inner, a.N);
       const float ar = cc.alpha_re, ai = cc.alpha_im;
       const float2 hs = divc(make_float2(0.f, ai), make_float2(ar, ai)) * a.inv_total;
