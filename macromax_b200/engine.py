@@ -38,6 +38,21 @@ def _ptr(t: torch.Tensor):
     return nat.device_ptr(t)
 
 
+def pack_symmetric(chi: torch.Tensor) -> tuple[torch.Tensor, int]:
+    """chi: [1 | 9, N] (a scalar or a row-major 3x3 per voxel).  Returns (chi, kind): a 3x3 that equals its transpose
+    exactly (every reciprocal medium: a symmetric permittivity, as in uniaxial grains) as its six distinct entries
+    xx, xy, xz, yy, yz, zz (MMX_CHI_SYM6), so the prologue and epilogue passes read 6 words per voxel instead of 9;
+    any other 3x3 as it is (MMX_CHI_MAT3); a scalar as it is (MMX_CHI_SCALAR)."""
+    m = int(chi.shape[0])
+    if m == 1:
+        return chi, nat.MMX_CHI_SCALAR
+    if m != 9:
+        raise ValueError('chi must hold 1 or 9 entries per voxel')
+    if torch.equal(chi[1], chi[3]) and torch.equal(chi[2], chi[6]) and torch.equal(chi[5], chi[7]):
+        return chi[list(nat.SYM6_ROWS)].contiguous(), nat.MMX_CHI_SYM6
+    return chi, nat.MMX_CHI_MAT3
+
+
 class IterationEngine:
     def __init__(self, shape, ncomp: int, batch: int, dtype, ks, chi0: np.ndarray, alpha0: complex,
                  device=None):
@@ -96,15 +111,7 @@ class IterationEngine:
         self._pack_symmetric()
 
     def _pack_symmetric(self):
-        """A 3x3 chi that equals its transpose (every reciprocal medium: a symmetric permittivity, as in the uniaxial
-        grains of the anisotropic workload) is kept as its six distinct entries (MMX_CHI_SYM6), so the prologue and
-        epilogue passes read 6 words per voxel instead of 9."""
-        if self.chi_kind != nat.MMX_CHI_MAT3:
-            return
-        c = self.chi
-        if torch.equal(c[1], c[3]) and torch.equal(c[2], c[6]) and torch.equal(c[5], c[7]):
-            self.chi = c[list(nat.SYM6_ROWS)].contiguous()
-            self.chi_kind = nat.MMX_CHI_SYM6
+        self.chi, self.chi_kind = pack_symmetric(self.chi)
 
     def rebase_alpha(self, chi0: np.ndarray, alpha0: complex, sources0: np.ndarray | None = None):
         """Install a new material (chi at alpha0) and reset every RHS's alpha to alpha0."""

@@ -23,6 +23,7 @@ import torch
 
 from . import _native as nat
 from .batch import BatchSolution, prepare_material
+from .engine import pack_symmetric
 from .grid import Grid
 
 
@@ -69,12 +70,7 @@ class MixedSolution:
                                                          requirements='W')).to(self.device)
             # a 3x3 chi equal to its transpose in FP64 is kept as its six distinct entries, as the inner
             # iteration keeps its complex64 copy
-            self.chi64_kind = eng.chi_kind if eng.chi_kind == nat.MMX_CHI_SCALAR else nat.MMX_CHI_MAT3
-            c = self.chi64
-            if self.chi64_kind == nat.MMX_CHI_MAT3 and torch.equal(c[1], c[3]) and torch.equal(c[2], c[6]) \
-                    and torch.equal(c[5], c[7]):
-                self.chi64 = c[list(nat.SYM6_ROWS)].contiguous()
-                self.chi64_kind = nat.MMX_CHI_SYM6
+            self.chi64, self.chi64_kind = pack_symmetric(self.chi64)
             # s'0 = i s / (alpha_i beta) in FP64, scaled on the device (one upload of the sources, no host copy when
             # they are already contiguous complex128)
             s_host = np.require(np.ascontiguousarray(src, dtype=np.complex128), requirements='W')

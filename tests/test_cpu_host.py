@@ -116,3 +116,33 @@ def test_device_ptr_refuses_strided_tensors():
     assert nat.device_ptr(t).value == t.data_ptr()
     with pytest.raises(ValueError):
         nat.device_ptr(t.t())
+
+
+def test_symmetric_chi_is_packed_to_six_entries():
+    """A 3x3 chi equal to its transpose is stored as xx, xy, xz, yy, yz, zz (MMX_CHI_SYM6); any other 3x3 and a
+    scalar are kept as they are.  The rows of the packed form expand back to the full matrix."""
+    import torch
+    from macromax_b200 import _native as nat
+    from macromax_b200.engine import pack_symmetric
+    rng = np.random.default_rng(9)
+    n = 50
+    a = rng.standard_normal((3, 3, n)) + 1j * rng.standard_normal((3, 3, n))
+    sym = torch.from_numpy((a + a.transpose(1, 0, 2)).reshape(9, n).astype(np.complex64))
+    packed, kind = pack_symmetric(sym)
+    assert kind == nat.MMX_CHI_SYM6 and tuple(packed.shape) == (6, n) and packed.is_contiguous()
+    full = torch.empty_like(sym)
+    for r, (i, j) in zip(range(6), ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))):
+        full[3 * i + j] = packed[r]
+        full[3 * j + i] = packed[r]
+    assert torch.equal(full, sym)
+    asym = torch.from_numpy(a.reshape(9, n).astype(np.complex64))
+    out, kind = pack_symmetric(asym)
+    assert kind == nat.MMX_CHI_MAT3 and out is asym
+    almost = sym.clone()
+    almost[5, 7] += 1e-6  # symmetric except one voxel of the yz / zy pair: not packed
+    assert pack_symmetric(almost)[1] == nat.MMX_CHI_MAT3
+    scalar = torch.ones((1, n), dtype=torch.complex64)
+    out, kind = pack_symmetric(scalar)
+    assert kind == nat.MMX_CHI_SCALAR and out is scalar
+    with pytest.raises(ValueError):
+        pack_symmetric(torch.ones((4, n), dtype=torch.complex64))
