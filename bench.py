@@ -1,7 +1,7 @@
 """
 Benchmark of the B200 split-Richardson iteration (voxel-iterations per second).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload spheres3d] [--n 128]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload spheres3d] [--n|--size 128]
 
 Workload (default): 3D vector Maxwell, isotropic, complex64, 128^3 grid, 200 seeded spheres, 12-voxel absorbing
 ramp, x-polarised Gaussian sheet source (macromax_b200.workloads.spheres_3d).  A step is one iteration
@@ -625,7 +625,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='spheres3d')
-    ap.add_argument('--n', type=int, default=128)
+    # --size: the same option under torchrun, whose own parser takes --n for an abbreviation of its options
+    ap.add_argument('--n', '--size', dest='n', type=int, default=128)
     ap.add_argument('--cpu-iters', type=int, default=6)
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
