@@ -146,3 +146,12 @@ def test_symmetric_chi_is_packed_to_six_entries():
     assert kind == nat.MMX_CHI_SCALAR and out is scalar
     with pytest.raises(ValueError):
         pack_symmetric(torch.ones((4, n), dtype=torch.complex64))
+
+
+def test_python_constants_match_header_defines():
+    """Every MMX_* value of the header's #define lines has the same value in the ctypes mirror."""
+    from macromax_b200 import _native as nat
+    defines = re.findall(r'^#define\s+(MMX_\w+)\s+\(?(-?\d+)u?\)?', open(HEADER).read(), flags=re.M)
+    assert len(defines) >= 15
+    for name, value in defines:
+        assert getattr(nat, name) == int(value), name
