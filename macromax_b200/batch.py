@@ -20,7 +20,7 @@ import torch
 
 from . import _native as nat
 from . import preconditioner as pc
-from .bound import Bound, Electric, PeriodicBound
+from .bound import Bound, PeriodicBound, is_electric
 from .engine import IterationEngine
 from .grid import Grid
 
@@ -38,7 +38,7 @@ def prepare_material(grid: Grid, epsilon, bound: Bound | None, wavenumber: float
     """Permittivity (plus an Electric bound's susceptibility) as a matrix field, and its preconditioner."""
     bound = bound if bound is not None else PeriodicBound(grid)
     eps = _to_matrix_field(np.asarray(epsilon, dtype=np.complex128), grid.ndim)
-    if isinstance(bound, Electric):
+    if is_electric(bound):
         chi_b = np.asarray(bound.electric_susceptibility)
         if eps.shape[0] > 1:
             chi_b = np.eye(3).reshape(3, 3, *([1] * grid.ndim)) * chi_b

@@ -1,7 +1,18 @@
 """
-Calculation-volume boundaries with the semantics of the reference ``macromax.bound`` (bound.py:19-215): a ``Bound``
-carries a thickness per axis and side (its smallest non-zero value biases alpha, solver.py:591-627); an ``Electric``
-bound adds its susceptibility to the permittivity before the preconditioner is built (solver.py:242-247).
+Calculation-volume boundaries, with the interface of the reference's ``macromax.bound`` (bound.py:19-215).
+
+What the iteration needs from a bound is small: its thickness per (axis, side), whose smallest non-zero value biases
+alpha (solver.py:591-627), and, for an absorbing bound, the susceptibility that is added to the permittivity before
+the preconditioner is built (solver.py:242-247).  Any object with ``thickness`` (and, for absorbing bounds,
+``electric_susceptibility``) is accepted by the solvers here, the reference's own bound objects included
+(``is_electric`` below).
+
+Absorbing layers are built separably.  Along one axis, a layer of thickness t on the front side reaches depth
+``t - d`` at a sample whose distance from the first sample is d (the back side: from the last sample); the relative
+depth ``(t - d) / t`` in (0, 1] is mapped through that side's extinction profile.  The axis's profile is the larger
+of its two sides, and the N-D extinction is the maximum over the axes' 1-D profiles, broadcast against each other
+(so corners take the largest of the overlapping layers, as in bound.py:158-183).  Axes without a layer contribute
+nothing, so the result keeps singleton dimensions there.
 """
 from __future__ import annotations
 
@@ -13,8 +24,19 @@ import numpy as np
 from .grid import Grid
 
 
+def is_electric(bound) -> bool:
+    """Whether ``bound`` carries an electric susceptibility: the ``Electric`` mixin here or in the reference
+    package (matched by class name, so the reference need not be importable)."""
+    return any(c.__name__ == 'Electric' for c in type(bound).__mro__)
+
+
+def is_magnetic(bound) -> bool:
+    """Whether ``bound`` carries a magnetic susceptibility (the ``Magnetic`` mixin, here or in the reference)."""
+    return any(c.__name__ == 'Magnetic' for c in type(bound).__mro__)
+
+
 class Electric:
-    """Marks a bound with a non-zero electric susceptibility."""
+    """Mixin: the bound has a non-zero electric susceptibility."""
 
     @property
     def background_permittivity(self) -> Complex:
@@ -26,24 +48,30 @@ class Electric:
 
     @property
     def permittivity(self) -> np.ndarray:
+        """Background permittivity plus the bound's susceptibility (may hold singleton dimensions)."""
         return self.background_permittivity + self.electric_susceptibility
 
 
 class Magnetic:
-    """Marks a bound with a non-zero magnetic susceptibility (magnetic media are not supported by this solver)."""
+    """Mixin: the bound has a non-zero magnetic susceptibility."""
 
     @property
     def magnetic_susceptibility(self) -> np.ndarray:
         return NotImplemented
 
+    @property
+    def permeability(self) -> np.ndarray:
+        return 1.0 + self.magnetic_susceptibility
+
 
 class Bound:
+    """A boundary of the calculation volume: thickness[axis, side] in the grid's length unit, side 0 at the first
+    sample of the axis and side 1 at the last."""
+
     def __init__(self, grid: Union[Grid, Sequence, np.ndarray, None] = None,
                  thickness: Union[Real, Sequence, np.ndarray] = 0.0, background_permittivity: Complex = 1.0):
-        if not isinstance(grid, Grid):
-            grid = Grid.from_ranges(grid)
-        self._grid = grid
-        self._thickness = np.broadcast_to(thickness, (grid.ndim, 2)).astype(float)
+        self._grid = grid if isinstance(grid, Grid) else Grid.from_ranges(grid)
+        self._thickness = np.array(np.broadcast_to(thickness, (self._grid.ndim, 2)), dtype=float)
         self._background_permittivity = background_permittivity
 
     @property
@@ -52,7 +80,6 @@ class Bound:
 
     @property
     def thickness(self) -> np.ndarray:
-        """Thickness [axis, front/back] in the grid's length unit."""
         return self._thickness.copy()
 
     @property
@@ -67,6 +94,32 @@ class Bound:
     def magnetic_susceptibility(self) -> np.ndarray:
         return np.zeros(self.grid.shape)
 
+    def _distances(self, axis: int) -> tuple[np.ndarray, np.ndarray]:
+        """Distance of every sample of ``axis`` from the first and from the last sample (both >= 0)."""
+        n = self.grid.shape[axis]
+        spacing = abs(float(np.asarray(self.grid.step)[axis]))
+        idx = np.arange(n, dtype=float)
+        return idx * spacing, (n - 1 - idx) * spacing
+
+    def _plaid(self, axis: int, profile: np.ndarray) -> np.ndarray:
+        shape = [1] * self.grid.ndim
+        shape[axis] = profile.size
+        return profile.reshape(shape)
+
+    @property
+    def between(self) -> np.ndarray:
+        """True where a sample lies inside the calculation volume proper (the inner edge of a layer included)."""
+        inside = np.asarray(True)
+        for axis in range(self.grid.ndim):
+            d_front, d_back = self._distances(axis)
+            keep = (d_front >= self._thickness[axis, 0]) & (d_back >= self._thickness[axis, 1])
+            inside = inside & self._plaid(axis, keep)
+        return inside
+
+    @property
+    def beyond(self) -> np.ndarray:
+        return ~self.between
+
 
 class PeriodicBound(Bound):
     def __init__(self, grid):
@@ -74,41 +127,73 @@ class PeriodicBound(Bound):
 
 
 class AbsorbingBound(Bound, Electric):
+    """Layers whose extinction coefficient kappa follows a profile of the relative depth (0 at the layer's inner edge,
+    1 at the edge of the volume); one profile per (axis, side), or one for all."""
+
     def __init__(self, grid, thickness=0.0,
                  extinction_coefficient_function: Union[Callable, Sequence, np.ndarray] = lambda rel_depth: rel_depth,
                  background_permittivity: Complex = 1.0):
         super().__init__(grid=grid, thickness=thickness, background_permittivity=background_permittivity)
-        self._kappa_functions = np.broadcast_to(np.asarray(extinction_coefficient_function, dtype=object),
-                                                (self.grid.ndim, 2))
+        profiles = np.empty((self.grid.ndim, 2), dtype=object)
+        profiles[...] = np.broadcast_to(np.asarray(extinction_coefficient_function, dtype=object),
+                                        (self.grid.ndim, 2))
+        self._profiles = profiles
+
+    @property
+    def is_electric(self) -> bool:
+        return True
+
+    def _axis_extinction(self, axis: int) -> np.ndarray | None:
+        """The larger of the axis's two layer profiles at every sample, or None where the axis has no layer."""
+        result = None
+        for side, dist in enumerate(self._distances(axis)):
+            t = self._thickness[axis, side]
+            depth = t - dist
+            inside = depth > 0
+            if not inside.any():
+                continue
+            rel_depth = np.where(inside, depth / t if t != 0 else 0.0, 0.0)
+            kappa = np.where(inside, np.asarray(self._profiles[axis, side](rel_depth), dtype=float), 0.0)
+            result = np.maximum(0.0 if result is None else result, kappa)
+        return result
 
     @property
     def extinction(self) -> np.ndarray:
-        """Extinction kappa on the plaid grid; maximum over overlapping axes at corners (bound.py:158-183)."""
         kappa = 0.0
-        for axis, rng in enumerate(self.grid):
-            for back in range(2):
-                t = self._thickness[axis, back] * np.sign(self.grid.step[axis])
-                if not back:
-                    depth = (rng.ravel()[0] + t) - rng
-                else:
-                    depth = rng - (rng.ravel()[-1] - t)
-                depth = depth * np.sign(self.grid.step[axis])
-                inside = depth > 0
-                if np.any(inside):
-                    rel = inside * depth / t
-                    kappa = np.maximum(kappa, self._kappa_functions[axis, back](rel) * inside)
+        for axis in range(self.grid.ndim):
+            prof = self._axis_extinction(axis)
+            if prof is not None:
+                kappa = np.maximum(kappa, self._plaid(axis, prof))
         return kappa
 
     @property
     def electric_susceptibility(self) -> np.ndarray:
+        """chi = (n + i kappa)^2 - eps_background with n the background's (principal) refractive index."""
         n = np.lib.scimath.sqrt(self.background_permittivity)
-        eps = (n + 1j * self.extinction) ** 2
-        return eps - self.background_permittivity
+        return (n + 1j * self.extinction) ** 2 - self.background_permittivity
 
 
 class LinearBound(AbsorbingBound):
+    """Extinction rising linearly with depth to ``max_extinction_coefficient`` (per axis and side, broadcast) at the
+    edge of the volume."""
+
     def __init__(self, grid, thickness=0.0, max_extinction_coefficient=0.25, background_permittivity: Complex = 1.0):
         self._max_extinction_coefficient = max_extinction_coefficient
-        funcs = np.vectorize(lambda kmax: (lambda rel: kmax * rel), otypes=[object])(max_extinction_coefficient)
-        super().__init__(grid=grid, thickness=thickness, extinction_coefficient_function=funcs,
+        grid_ = grid if isinstance(grid, Grid) else Grid.from_ranges(grid)
+        peaks = np.broadcast_to(np.asarray(max_extinction_coefficient, dtype=float), (grid_.ndim, 2))
+        profiles = np.empty((grid_.ndim, 2), dtype=object)
+        for axis in range(grid_.ndim):
+            for side in range(2):
+                profiles[axis, side] = _Linear(float(peaks[axis, side]))
+        super().__init__(grid=grid_, thickness=thickness, extinction_coefficient_function=profiles,
                          background_permittivity=background_permittivity)
+
+
+class _Linear:
+    """kappa(rel_depth) = peak * rel_depth."""
+
+    def __init__(self, peak: float):
+        self.peak = peak
+
+    def __call__(self, rel_depth):
+        return self.peak * rel_depth

@@ -25,7 +25,8 @@ import scipy.optimize
 import torch
 
 from . import _native as nat
-from .bound import Electric, Magnetic, PeriodicBound
+from .bound import PeriodicBound, is_electric
+from .bound import is_magnetic as has_magnetic_bound
 from .grid import Grid
 from .preconditioner import has_gain, increase_bias
 
@@ -74,7 +75,7 @@ def needs_magnetic_solver(grid, epsilon=None, xi=0.0, zeta=0.0, mu=1.0, refracti
         return f(*grid) if callable(f) else np.asarray(f)
 
     mu_arr = func2arr(mu)
-    if isinstance(bound, Magnetic) and np.any(np.asarray(bound.magnetic_susceptibility) != 0):
+    if has_magnetic_bound(bound) and np.any(np.asarray(bound.magnetic_susceptibility) != 0):
         return True
     if epsilon is None and refractive_index is not None:
         n = _matrix_field(func2arr(refractive_index), grid.ndim)
@@ -206,10 +207,10 @@ class MagneticSolution:
         epsilon = _matrix_field(func2arr(epsilon), ndim)
         mu = _matrix_field(mu, ndim)
         eye = np.eye(3).reshape(3, 3, *([1] * ndim))
-        if isinstance(self._bound, Electric):
+        if is_electric(self._bound):
             chi_b = np.asarray(self._bound.electric_susceptibility)
             epsilon = epsilon + (eye * chi_b if not _is_scalar(epsilon) else chi_b)
-        if isinstance(self._bound, Magnetic):
+        if has_magnetic_bound(self._bound):
             chi_b = np.asarray(self._bound.magnetic_susceptibility)
             mu = mu + (eye * chi_b if not _is_scalar(mu) else chi_b)
         self._pre = MagneticPreconditioner(epsilon, func2arr(xi), func2arr(zeta), mu, grid.step, self._wavenumber,

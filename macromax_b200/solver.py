@@ -20,7 +20,7 @@ import scipy.constants as const
 
 from . import _native as nat
 from . import preconditioner as pc
-from .bound import Bound, Electric, Magnetic, PeriodicBound
+from .bound import Bound, PeriodicBound, is_electric, is_magnetic
 from .engine import IterationEngine
 from .grid import Grid
 
@@ -107,7 +107,7 @@ class Solution:
         if not (np.allclose(func2arr(xi), 0) and np.allclose(func2arr(zeta), 0)
                 and np.allclose(mu_arr, np.ravel(mu_arr)[0]) and np.asarray(mu_arr).ndim <= self._grid.ndim):
             raise NotImplementedError('magnetic or bi-anisotropic media are not supported by the B200 backend')
-        if isinstance(self._bound, Magnetic) and np.any(self._bound.magnetic_susceptibility != 0):
+        if is_magnetic(self._bound) and np.any(self._bound.magnetic_susceptibility != 0):
             raise NotImplementedError('magnetic boundaries are not supported by the B200 backend')
         self._mu = complex(np.ravel(mu_arr)[0])
         if epsilon is None:
@@ -117,7 +117,7 @@ class Solution:
             if n.shape[0] == 1 and np.any(n.real < 0):
                 raise NotImplementedError('negative refractive index (magnetic) media are not supported')
         epsilon = self._to_matrix_field(np.asarray(func2arr(epsilon), dtype=np.complex128))
-        if isinstance(self._bound, Electric):
+        if is_electric(self._bound):
             chi_b = np.asarray(self._bound.electric_susceptibility)
             if epsilon.shape[0] > 1:
                 chi_b = np.eye(3).reshape(3, 3, *([1] * self._grid.ndim)) * chi_b
@@ -228,7 +228,7 @@ class Solution:
     @property
     def epsilon(self) -> np.ndarray:
         eps = self._eps_field
-        if isinstance(self._bound, Electric):
+        if is_electric(self._bound):
             chi_b = np.asarray(self._bound.electric_susceptibility)
             if eps.shape[0] > 1:
                 chi_b = np.eye(3).reshape(3, 3, *([1] * self._grid.ndim)) * chi_b
@@ -239,7 +239,7 @@ class Solution:
     def epsilon(self, new_value):
         """solver.py:755-787: new material, same source and field; the preconditioner is rebuilt."""
         eps = self._to_matrix_field(np.asarray(new_value, dtype=np.complex128))
-        if isinstance(self._bound, Electric):
+        if is_electric(self._bound):
             chi_b = np.asarray(self._bound.electric_susceptibility)
             if eps.shape[0] > 1:
                 chi_b = np.eye(3).reshape(3, 3, *([1] * self._grid.ndim)) * chi_b

@@ -4,7 +4,9 @@ Import the reference ``macromax`` package for fixture generation (and for the op
 The reference package writes a log file next to itself on import (``macromax/__init__.py:61-67``) and needs
 ``coloredlogs`` and installed package metadata, neither of which exists here.  So this helper copies the package to
 a temporary directory, puts a minimal ``coloredlogs`` stand-in on ``sys.path`` and answers the version lookup.
-It reads the reference tree, so it is only usable where that tree exists; nothing that runs on a GPU box uses it.
+The package is looked up in ``$MACROMAX_REFERENCE`` (a directory holding ``macromax/``) and otherwise in the
+repository's ``baseline/_ref`` (the reference package placed there for the reference arm; not part of the
+repository's history).  Where neither exists, ``reference_available()`` is False and the tests that need it skip.
 """
 from __future__ import annotations
 
@@ -15,7 +17,8 @@ import shutil
 import sys
 import tempfile
 
-REFERENCE_PYTHON = os.environ.get('MACROMAX_REFERENCE', '/root/reference/python')
+_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+REFERENCE_PYTHON = os.environ.get('MACROMAX_REFERENCE', os.path.join(_REPO, 'baseline', '_ref'))
 
 _STUB = '''
 import logging

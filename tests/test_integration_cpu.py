@@ -63,3 +63,41 @@ def test_grid_and_bound_conventions_match_reference():
     kb = LinearBound(g, thickness=1.0, max_extinction_coefficient=0.3).electric_susceptibility
     kr = RefLinearBound(g_ref, thickness=1.0, max_extinction_coefficient=0.3).electric_susceptibility
     assert np.allclose(np.broadcast_to(kb, g.shape), np.broadcast_to(kr, g.shape), rtol=1e-14, atol=1e-14)
+
+
+@pytest.mark.parametrize('thickness, kmax, bg', [
+    (1.0, 0.3, 1.0),
+    ([[0.5, 1.25], [0.0, 2.0], [1.0, 0.0]], [[0.1, 0.2], [0.3, 0.4], [0.5, 0.6]], 2.25),
+    ([[0.0], [1.5], [0.0]], 0.25, 1.0 + 0.1j),
+    (0.0, 0.25, 1.0),
+])
+def test_bounds_match_reference_3d(thickness, kmax, bg):
+    """Extinction, susceptibility, between/beyond and thickness of the bounds equal the reference classes'
+    (bound.py:55-215) on a 3D grid with per-(axis, side) thicknesses and peaks, including axes without layers."""
+    mm = _reference()
+    from macromax import bound as rb
+    from macromax_b200 import AbsorbingBound, Bound, Grid, LinearBound
+    g_ref = mm.Grid([10, 16, 12], [0.25, 0.5, 0.125])
+    g = Grid(shape=(10, 16, 12), step=(0.25, 0.5, 0.125))
+    ours, ref = LinearBound(g, thickness, kmax, bg), rb.LinearBound(g_ref, thickness, kmax, bg)
+    assert np.array_equal(ours.thickness, ref.thickness)
+    k_o, k_r = np.asarray(ours.extinction), np.asarray(ref.extinction)
+    assert k_o.shape == k_r.shape
+    assert np.allclose(k_o, k_r, rtol=1e-14, atol=1e-15)
+    assert np.allclose(ours.electric_susceptibility, ref.electric_susceptibility, rtol=1e-14, atol=1e-15)
+    assert np.array_equal(np.broadcast_to(ours.between, g.shape), np.broadcast_to(ref.between, g.shape))
+    assert np.array_equal(np.broadcast_to(ours.beyond, g.shape), np.broadcast_to(ref.beyond, g.shape))
+    fn = (lambda r: r ** 2)
+    a_o, a_r = AbsorbingBound(g, thickness, fn, bg), rb.AbsorbingBound(g_ref, thickness, fn, bg)
+    assert np.allclose(a_o.extinction, a_r.extinction, rtol=1e-14, atol=1e-15)
+    assert np.array_equal(Bound(g, thickness).thickness, rb.Bound(g_ref, thickness).thickness)
+
+
+def test_solver_accepts_reference_bound_objects():
+    """The reference's own bound objects count as electric bounds here (duck typing on the mixin)."""
+    mm = _reference()
+    from macromax import bound as rb
+    from macromax_b200.bound import is_electric, is_magnetic
+    g_ref = mm.Grid([8, 8], 0.25)
+    assert is_electric(rb.LinearBound(g_ref, 0.5)) and not is_electric(rb.Bound(g_ref, 0.5))
+    assert not is_magnetic(rb.LinearBound(g_ref, 0.5))
