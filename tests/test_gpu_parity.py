@@ -75,6 +75,37 @@ def test_c64_device_stop_rule_converges_like_reference(name):
     assert rel(sol.E, z['final']) < 1e-4
 
 
+def test_full_size_disks2d_256_c128_all_500_iterations():
+    """The complex128 configuration at its full size (256^2, 20 disks, 500 iterations).  The fixture keeps the
+    reference's residue and update norm of every iteration in FP64 and its fields in complex64 (inputs come from the
+    seeded generator, checked against the fixture's checksums)."""
+    from macromax_b200 import Bound, Grid, Solution, workloads
+    z = load_golden('disks2d_256_c128')
+    wl = workloads.disks_2d(n=256, seed=1)
+    eps = wl['epsilon']
+    assert np.isclose(np.sum(np.abs(eps) * np.arange(eps.size).reshape(eps.shape) % 1009),
+                      float(z['epsilon_checksum']), rtol=1e-12)
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=eps, source_distribution=wl['source'],
+                   bound=Bound(grid, thickness=wl['bound_thickness']), dtype=np.complex128)
+    assert abs(sol.alpha - complex(z['alpha0'])) <= 1e-12 * abs(complex(z['alpha0']))
+    residues, norms, fields = [], [], {}
+    for s in sol:
+        residues.append(s.residue)
+        norms.append(s.previous_update_norm)
+        if s.iteration in (1, 20):
+            fields[s.iteration] = s.E
+        if not (s.iteration < int(z['maxiter']) and s.residue > float(z['rtol'])):
+            break
+    assert sol.iteration == int(z['iterations']) == 500
+    np.testing.assert_allclose(residues, z['residues'], rtol=1e-10)
+    np.testing.assert_allclose(norms, z['update_norms'], rtol=1e-10)
+    assert sol.rejections == int(np.sum(np.diff(z['alphas']) != 0))
+    for it in (1, 20):  # the fixture's fields are stored in complex64
+        assert rel(fields[it], z[f'E_{it}']) < 1e-7, it
+    assert rel(sol.E, z['final']) < 1e-7
+
+
 def test_c128_device_stop_rule_iteration_count_is_exact():
     z = load_golden('disks2d_64_c128')
     sol = solution_from_golden(z, np.complex128)
