@@ -359,13 +359,16 @@ class BackEndB200:
 
 def register(macromax_module=None):
     """
-    Add the ``'b200'`` type to the reference's ``macromax.backend.load`` (backend/__init__.py:922-1012): a config
-    ``{'type': 'b200', 'device': 'cuda:0'}`` builds a ``BackEndB200``; when the GPU or the native library is missing
-    the constructor raises ``ImportError`` and ``load`` moves on to the next configured backend, as it does for its
-    own types.  Returns the wrapped ``load``.
+    Add the ``'b200'`` type to the reference's ``macromax.backend.load`` (backend/__init__.py:922-1012) and route the
+    reference's ``Solution`` iteration to the fused kernels for it (``refhook.install``).  A config
+    ``{'type': 'b200', 'device': 'cuda:0'}`` builds the reference-facing ``BackEndB200`` (a subclass of the
+    reference's torch backend, ``refhook.backend_class``); when the GPU or the native library is missing the
+    constructor raises ``ImportError`` and ``load`` moves on to the next configured backend, as it does for its own
+    types.  Returns the wrapped ``load``.
     """
     if macromax_module is None:
         import macromax as macromax_module  # the reference package
+    from . import refhook
     be = macromax_module.backend
     original = getattr(be.load, '_b200_original', be.load)
 
@@ -379,8 +382,7 @@ def register(macromax_module=None):
         for i, c in enumerate(configs):
             if str(c.get('type', '')).lower() == 'b200':
                 try:
-                    return BackEndB200(nb_pol_dims, Grid(shape=grid.shape, step=grid.step), dtype,
-                                       device=c.get('device'))
+                    return refhook.backend_class(macromax_module)(nb_pol_dims, grid, dtype, device=c.get('device'))
                 except ImportError as ie:
                     be.log.info(f'Backend type "b200" did not load as expected: {ie}.')
                     continue
@@ -390,4 +392,5 @@ def register(macromax_module=None):
 
     load._b200_original = original
     be.load = load
+    refhook.install(macromax_module)
     return load

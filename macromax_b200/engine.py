@@ -196,7 +196,8 @@ class IterationEngine:
     def run(self, rtol: float, maxiter: float, chunk: int = 8, max_chunk: int = 64,
             reset_iteration: bool = True) -> np.ndarray:
         """Iterate every active RHS until its stop rule (iteration < maxiter and residue > rtol) fails; the iteration
-        count starts from 0, or goes on from its current value (reset_iteration=False, as Solution.solve does)."""
+        count starts from 0 (as every Solution.solve, solver.py:1063), or goes on from its current value
+        (reset_iteration=False)."""
         st = self.read_state()
         if reset_iteration:
             st['iteration'] = 0

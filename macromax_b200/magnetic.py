@@ -371,8 +371,9 @@ class MagneticSolution:
             raise ZeroDivisionError('float division by zero')
 
     def __iter__(self):
-        """solver.py:1049-1098: every next() runs one iteration on the device."""
-        self._set_state(rtol=-1.0, maxiter=inf, active=1, status=0)
+        """solver.py:1049-1098: every next() runs one iteration on the device; obtaining the iterator resets the
+        iteration count (solver.py:1063)."""
+        self._set_state(rtol=-1.0, maxiter=inf, active=1, status=0, iteration=0)
         while True:
             self._run(1)
             self._check(self._read_state()[0])
@@ -389,7 +390,7 @@ class MagneticSolution:
                 if not callback(sol):
                     break
             return self
-        self._set_state(rtol=float(rtol), maxiter=float(maxiter), active=1, status=0)
+        self._set_state(rtol=float(rtol), maxiter=float(maxiter), active=1, status=0, iteration=0)
         while True:
             self._run(chunk)
             st = self._read_state()[0]

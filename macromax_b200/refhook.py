@@ -1,0 +1,297 @@
+"""
+The reference package's own ``Solution`` on the fused B200 iteration.
+
+``install(mm)`` (called by ``macromax_b200.backend.register``) does two things to an importable reference package
+``mm``:
+
+1. It defines the reference-facing backend class: ``BackEndB200`` derived from the reference's ``BackEndTorch``
+   (itself a ``BackEnd``, backend/__init__.py:37-880), so every per-op method keeps the reference's semantics on
+   device tensors, while ``ft``, ``ift``, ``norm`` and ``curl_ft`` run on this library's kernels (``mmx_fftn``,
+   ``mmx_norm``, ``mmx_curl_ft``).  ``backend.load`` builds it for ``{'type': 'b200'}``.
+2. It replaces ``Solution.__iter__`` and ``Solution.solve`` (solver.py:1049-1123) with versions that, when the
+   solution's backend is that class and the medium is not magnetic, run the whole iteration body
+   (solver.py:1070-1096: chi, source, Green function, chi, norm, divergence guard, update) as the fused pass
+   kernels of ``mmx_iterate``; any other backend or a magnetic medium runs the reference's own code unchanged.
+
+The operator data is read from the solution's private attributes, as the reference stores them:
+``_Solution__chiEE_base`` and ``_Solution__source_normalized`` (both at the current alpha, solver.py:474-486),
+``_Solution__alpha``, ``_Solution__field_array`` (E x k0^2) and ``_Solution__previous_update_norm``.  Before every
+step the hook compares them with what the device engine holds (tensor identity, in-place version counter, alpha), so
+a new field (the ``E`` setter), source or permittivity set between iterations is picked up.  After a step the
+solution's field attribute is pointed at the engine's current buffer (no copy), its update norm and residue are
+set from the device state, and a raised alpha (divergence guard) is passed to the reference's own
+``_Solution__update_operators``, so the solution's stored operators stay what the reference would hold.
+
+``solve`` with ``callback=None`` (``rtol`` / ``maxiter``) or with the reference's default callback (iteration < 1e4
+and residue > 1e-4, the defaults of ``Solution.solve`` and ``macromax.solve``) runs in device-side chunks with the
+stop rule checked after every iteration on the device; any other callback is called after every fused iteration.
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib
+import math
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .engine import IterationEngine
+
+_CLASSES = {}
+
+
+def _stream():
+    s = torch.cuda.current_stream().cuda_stream
+    return ctypes.c_void_p(s) if s else None
+
+
+def backend_class(mm):
+    """The reference-facing ``BackEndB200`` for the reference package ``mm`` (one class per package object)."""
+    key = id(mm)
+    if key in _CLASSES:
+        return _CLASSES[key]
+    BackEndTorch = importlib.import_module(mm.__name__ + '.backend.torch').BackEndTorch
+
+    class BackEndB200(BackEndTorch):
+        """The reference's torch backend on a B200, with the transforms, norms and curl on the native kernels."""
+
+        b200_fused = True  # Solution.__iter__ / solve take the fused iteration for this backend
+
+        def __init__(self, nb_dims: int, grid, hardware_dtype=torch.complex128, device: str | None = None):
+            if not torch.cuda.is_available():
+                raise ImportError('BackEndB200 needs a CUDA device')
+            nat.load()  # ImportError when the native library is missing: backend.load falls through
+            super().__init__(nb_dims, grid, hardware_dtype=hardware_dtype, device=device or 'cuda')
+            if self.hardware_dtype not in (torch.complex64, torch.complex128):
+                raise TypeError(f'unsupported dtype {hardware_dtype}: use complex64 or complex128')
+            self._b200_prec = nat.MMX_C64 if self.hardware_dtype == torch.complex64 else nat.MMX_C128
+            self._b200_shape = tuple(int(s) for s in grid.shape)
+            with torch.cuda.device(self._b200_device):
+                self._b200_plan = nat.Plan(self._b200_shape, 1, 1, self._b200_prec)
+                self._b200_plan.set_kvectors([np.asarray(k, dtype=np.float64).ravel() for k in grid.k])
+                self._b200_norm = torch.zeros(1, dtype=torch.float64, device=self._b200_device)
+
+        @property
+        def _b200_device(self) -> torch.device:
+            return self._BackEndTorch__device
+
+        def _native_grid_array(self, arr) -> bool:
+            nd = len(self._b200_shape)
+            return (isinstance(arr, torch.Tensor) and arr.dim() >= nd and arr.dtype == self.hardware_dtype
+                    and tuple(arr.shape[-nd:]) == self._b200_shape and arr.device == self._b200_device)
+
+        def _b200_fft(self, arr, inverse: int):
+            x = arr.contiguous()
+            nb = int(np.prod(x.shape[:-len(self._b200_shape)])) if x.dim() > len(self._b200_shape) else 1
+            out = torch.empty_like(x)
+            nat.call('mmx_fftn', self._b200_plan.handle, nat.device_ptr(x), nat.device_ptr(out), nb, int(inverse),
+                     _stream())
+            return out
+
+        def ft(self, arr):
+            """backend/torch.py:183-193: forward, unscaled FFT over the spatial axes (native mmx_fftn for arrays that
+            span the grid)."""
+            arr = self.astype(arr)
+            return self._b200_fft(arr, 0) if self._native_grid_array(arr) else super().ft(arr)
+
+        def ift(self, arr):
+            """backend/torch.py:195-205: inverse FFT scaled by 1/N (native mmx_fftn for arrays spanning the grid)."""
+            arr = self.astype(arr)
+            return self._b200_fft(arr, 1) if self._native_grid_array(arr) else super().ift(arr)
+
+        def norm(self, arr) -> float:
+            """backend/torch.py:316-317 on the FP64-accumulated native reduction (mmx_norm)."""
+            arr = self.astype(arr)
+            if not (arr.is_complex() and arr.device == self._b200_device):
+                return super().norm(arr)
+            x = arr.contiguous()
+            nat.call('mmx_norm', self._b200_plan.handle, nat.device_ptr(x), x.numel(), self._b200_prec,
+                     nat.device_ptr(self._b200_norm), _stream())
+            return float(self._b200_norm.item())
+
+        def curl_ft(self, F):
+            """backend/__init__.py:483-509: i k x F (native mmx_curl_ft for a 3-component field of this grid)."""
+            F = self.astype(F)
+            if self.vector_length == 3 and F.shape[0] == 3 and self._native_grid_array(F) \
+                    and F.numel() == 3 * int(np.prod(self._b200_shape)):
+                x = F.contiguous()
+                out = torch.empty_like(x)
+                nat.call('mmx_curl_ft', self._b200_plan.handle, nat.device_ptr(x), nat.device_ptr(out), _stream())
+                return out
+            return super().curl_ft(F)
+
+        def __str__(self):
+            return f'BackEndB200(vectorial={self.vectorial}, grid shape {self._b200_shape}, {self.hardware_dtype})'
+
+    BackEndB200.__module__ = __name__
+    BackEndB200.__qualname__ = 'BackEndB200'
+    _CLASSES[key] = BackEndB200
+    return BackEndB200
+
+
+def _matrix_rows(t: torch.Tensor, shape) -> torch.Tensor:
+    """[r, c, *grid-broadcastable] -> a new [r*c, N] tensor (broadcast over singleton grid dimensions).  Always a
+    copy: the reference rescales its operators in place when alpha changes, while the engine keeps chi at the alpha
+    it was given and maps it to the current alpha itself."""
+    r, c = int(t.shape[0]), int(t.shape[1])
+    return t.expand(r, c, *shape).reshape(r * c, int(np.prod(shape))).clone(memory_format=torch.contiguous_format)
+
+
+def _field_rows(t: torch.Tensor, ncomp: int, shape) -> torch.Tensor:
+    """A vector field [c | 1, 1, *grid-broadcastable] -> [ncomp, N] (a single row is repeated over components)."""
+    return t.expand(ncomp, 1, *shape).reshape(ncomp, int(np.prod(shape))).contiguous()
+
+
+def _stop_rule(callback, mm, default_callbacks):
+    """(rtol, maxiter) when ``callback`` is one of the reference's stop rules of that form, else None: its default
+    callbacks (iteration < 1e4 and residue > 1e-4) and the closure that ``macromax.solve(..., callback=None)``
+    builds from its rtol and maxiter arguments (solver.py:81-83)."""
+    if callback is None:
+        return None
+    if any(callback is d for d in default_callbacks):
+        return 1e-4, 1e4
+    code = getattr(callback, '__code__', None)
+    if (code is not None and getattr(callback, '__module__', None) == mm.solver.__name__
+            and callback.__qualname__ == 'solve.<locals>.callback' and callback.__closure__ is not None
+            and sorted(code.co_freevars) == ['maxiter', 'rtol']):
+        cells = dict(zip(code.co_freevars, (c.cell_contents for c in callback.__closure__)))
+        return float(cells['rtol']), float(cells['maxiter'])
+    return False
+
+
+class _FusedRunner:
+    """The device engine behind one reference ``Solution`` and the bookkeeping that keeps the two in step."""
+
+    def __init__(self, sol):
+        be = sol._Solution__BE
+        self.shape = tuple(int(s) for s in be.grid.shape)
+        self.ncomp = int(be.vector_length)
+        dtype = np.complex64 if be.hardware_dtype == torch.complex64 else np.complex128
+        alpha = complex(sol._Solution__alpha)
+        chi = _matrix_rows(sol._Solution__chiEE_base, self.shape)
+        self.engine = IterationEngine(self.shape, self.ncomp, 1, dtype,
+                                      [np.asarray(k, dtype=np.float64).ravel() for k in be.grid.k], chi, alpha,
+                                      device=be._b200_device)
+        self.material_key = None
+        self.field_key = None
+        self.prev_norm = None
+        self.iterations = 0  # fused iterations run for this solution (all calls)
+
+    @staticmethod
+    def _key(t):
+        return id(t), t._version, t.data_ptr()
+
+    def sync_in(self, sol):
+        """Bring the engine up to date with the solution's operators, field and update norm."""
+        eng = self.engine
+        chi, src = sol._Solution__chiEE_base, sol._Solution__source_normalized
+        alpha = complex(sol._Solution__alpha)
+        key = (self._key(chi), self._key(src), alpha)
+        st = None
+        if key != self.material_key:  # chi and the source are stored at the current alpha: rebase the engine there
+            eng.set_chi(_matrix_rows(chi, self.shape), alpha)
+            eng.set_sources(_field_rows(src, self.ncomp, self.shape))
+            st = eng.read_state()
+            st['alpha_re'] = st['alpha0_re'] = alpha.real
+            st['alpha_im'] = st['alpha0_im'] = alpha.imag
+            self.material_key = key
+        E = sol._Solution__field_array
+        if self._key(E) != self.field_key:
+            field = _field_rows(E, self.ncomp, self.shape)
+            st = eng.read_state() if st is None else st
+            eng.fields[int(st['cur'][0]), 0].copy_(field)
+            self.field_key = None
+        prev = float(sol._Solution__previous_update_norm)
+        if prev != self.prev_norm or st is not None:
+            st = eng.read_state() if st is None else st
+            st['prev_norm'] = prev
+            self.prev_norm = prev
+        if st is not None:
+            eng.write_state(st)
+
+    def sync_out(self, sol, st):
+        """Point the solution at the engine's current field and copy back the update norm, residue and alpha."""
+        cur = int(st['cur'][0])
+        view = self.engine.fields[cur, 0].view(self.ncomp, 1, *self.shape)
+        sol._Solution__field_array = view
+        self.field_key = self._key(view)
+        prev = float(st['prev_norm'][0])
+        sol._Solution__previous_update_norm = prev
+        self.prev_norm = prev
+        sol._Solution__relative_residue = float(st['residue'][0]) if prev > 0 else 0.0
+        alpha = complex(float(st['alpha_re'][0]), float(st['alpha_im'][0]))
+        if alpha != complex(sol._Solution__alpha):
+            # the divergence guard raised alpha on the device: let the reference rescale its own operators
+            sol._Solution__update_operators(alpha)
+            chi, src = sol._Solution__chiEE_base, sol._Solution__source_normalized
+            self.material_key = (self._key(chi), self._key(src), alpha)  # the engine maps chi0 to alpha itself
+        if int(st['status'][0]) == nat.MMX_STATUS_ZERODIV:
+            raise ZeroDivisionError('float division by zero')
+
+
+def _runner(sol) -> _FusedRunner:
+    r = sol.__dict__.get('_b200_runner')
+    if r is None:
+        r = _FusedRunner(sol)
+        sol.__dict__['_b200_runner'] = r
+    return r
+
+
+def _fused(sol) -> bool:
+    return getattr(sol._Solution__BE, 'b200_fused', False) and not sol.magnetic
+
+
+def install(mm):
+    """Route the reference ``Solution`` of package ``mm`` to the fused iteration for ``BackEndB200`` (idempotent)."""
+    Solution = mm.solver.Solution
+    if getattr(Solution, '_b200_hooked', False):
+        return
+    reference_iter, reference_solve = Solution.__iter__, Solution.solve
+    default_callbacks = tuple(f.__defaults__[0] for f in (reference_solve,) if f.__defaults__) + \
+        tuple(d for d in (mm.solver.solve.__defaults__ or ()) if callable(d))
+
+    def __iter__(self):
+        """solver.py:1049-1098; one fused iteration per next() on a BackEndB200."""
+        if not _fused(self):
+            yield from reference_iter(self)
+            return
+        runner = _runner(self)
+        eng = runner.engine
+        self.iteration = 0  # reset iteration counter (solver.py:1063)
+        st = eng.read_state()
+        st['rtol'], st['maxiter'], st['active'], st['status'] = -1.0, np.inf, 1, 0
+        eng.write_state(st)
+        while True:
+            self.iteration += 1
+            runner.sync_in(self)
+            eng.iterate(1)
+            runner.iterations += 1
+            runner.sync_out(self, eng.read_state())
+            yield self
+
+    def solve(self, callback=reference_solve.__defaults__[0], rtol: float = 0, maxiter=math.inf):
+        """solver.py:1100-1123; stop rules of the rtol/maxiter form run on the device in chunks."""
+        if not _fused(self):
+            return reference_solve(self, callback, rtol, maxiter)
+        rule = _stop_rule(callback, mm, default_callbacks)
+        if rule is False:
+            for _ in self:
+                if not callback(self):
+                    break
+            return self
+        if rule is not None:
+            rtol, maxiter = rule
+        runner = _runner(self)
+        runner.sync_in(self)
+        st = runner.engine.run(float(rtol), float(maxiter), reset_iteration=True)
+        runner.iterations += int(st['iteration'][0])
+        self.iteration = int(st['iteration'][0])
+        runner.sync_out(self, st)
+        return self
+
+    Solution.__iter__ = __iter__
+    Solution.solve = solve
+    Solution._b200_hooked = True
+    Solution._b200_reference_iter = reference_iter
+    Solution._b200_reference_solve = reference_solve

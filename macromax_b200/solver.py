@@ -321,9 +321,11 @@ class Solution:
 
     # -- iteration --------------------------------------------------------------------------------------------------
     def __iter__(self):
-        """solver.py:1049-1098: every next() runs one fused iteration on the device; the iteration count goes on
-        from its current value, and a zero update norm after a zero one raises ZeroDivisionError (solver.py:1079)."""
+        """solver.py:1049-1098: every next() runs one fused iteration on the device; obtaining the iterator resets the
+        iteration count (solver.py:1063), and a zero update norm after a zero one raises ZeroDivisionError
+        (solver.py:1079)."""
         st = self._engine.read_state()
+        st['iteration'] = 0
         st['rtol'] = -1.0
         st['maxiter'] = np.inf
         st['active'] = 1
@@ -340,7 +342,7 @@ class Solution:
         if callback is None or callback is _default_callback:
             if callback is _default_callback:
                 rtol, maxiter = 1e-4, 1e4
-            st = self._engine.run(float(rtol), float(maxiter), reset_iteration=False)
+            st = self._engine.run(float(rtol), float(maxiter), reset_iteration=True)
             self._check_status(st[0])
             return self
         for sol in self:

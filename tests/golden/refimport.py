@@ -66,3 +66,22 @@ def import_reference():
         if isinstance(h, logging.FileHandler):
             mm.log.removeHandler(h)
     return mm
+
+
+def reference_tests_dir() -> str | None:
+    """The reference's own test directory (``tests/`` beside the package), or None where it is absent."""
+    d = os.path.join(REFERENCE_PYTHON, 'tests')
+    return d if os.path.isfile(os.path.join(d, 'test_backend.py')) else None
+
+
+def load_reference_test_module(name: str):
+    """Import one of the reference's test modules (e.g. ``test_backend``) against the imported reference copy."""
+    import importlib.util
+    d = reference_tests_dir()
+    if d is None:
+        raise ImportError('the reference test directory is not present')
+    import_reference()
+    spec = importlib.util.spec_from_file_location(f'_reference_tests_{name}', os.path.join(d, f'{name}.py'))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod

@@ -101,3 +101,58 @@ def test_solver_accepts_reference_bound_objects():
     g_ref = mm.Grid([8, 8], 0.25)
     assert is_electric(rb.LinearBound(g_ref, 0.5)) and not is_electric(rb.Bound(g_ref, 0.5))
     assert not is_magnetic(rb.LinearBound(g_ref, 0.5))
+
+
+def test_hooked_reference_solution_is_unchanged_on_other_backends():
+    """With the fused-iteration hook installed, a reference Solution on the NumPy backend runs the reference's own
+    iteration: its residues equal the fixture the reference made (to rounding: 1e-13)."""
+    from conftest import load_golden
+    mm = _reference()
+    from macromax_b200.backend import register
+    register(mm)
+    assert getattr(mm.solver.Solution, '_b200_hooked', False)
+    mm.backend.config({'type': 'numpy'})
+    z = load_golden('disks2d_64_c128')
+    grid = mm.Grid(shape=tuple(int(s) for s in z['shape']), step=float(z['step']))
+    sol = mm.Solution(grid, vacuum_wavelength=float(z['wavelength']), epsilon=z['epsilon'],
+                      source_distribution=z['source'], bound=mm.bound.Bound(grid, thickness=float(z['bound_thickness'])),
+                      dtype=np.complex128)
+    residues = []
+    for s in sol:
+        residues.append(s.residue)
+        if s.iteration >= 30:
+            break
+    np.testing.assert_allclose(residues, z["residues"][:30], rtol=1e-13)
+    sol.solve(None, rtol=0, maxiter=7)
+    assert sol.iteration == 7  # the reference resets the count on every solve (solver.py:1063)
+
+
+def test_stop_rule_recognition():
+    """The hook runs on the device only the stop rules of the form iteration < maxiter and residue > rtol: the
+    reference's default callbacks and the closure macromax.solve(callback=None) builds; other callbacks run per
+    iteration on the host."""
+    mm = _reference()
+    from macromax_b200 import refhook
+    defaults = (mm.solver.Solution.solve.__defaults__[0] if not getattr(mm.solver.Solution, '_b200_hooked', False)
+                else mm.solver.Solution._b200_reference_solve.__defaults__[0],)
+    assert refhook._stop_rule(None, mm, defaults) is None
+    assert refhook._stop_rule(defaults[0], mm, defaults) == (1e-4, 1e4)
+    assert refhook._stop_rule(lambda s: s.iteration < 3, mm, defaults) is False
+    captured = {}
+
+    class Stop(Exception):
+        pass
+
+    def fake_solve(self, callback):
+        captured['cb'] = callback
+        raise Stop
+
+    orig = mm.solver.Solution.solve
+    try:
+        mm.solver.Solution.solve = fake_solve
+        with pytest.raises(Stop):
+            mm.solve(np.arange(8) * 0.1, vacuum_wavelength=1.0, source_distribution=np.ones((1, 8)), epsilon=1.0,
+                     callback=None, rtol=1e-7, maxiter=123)
+    finally:
+        mm.solver.Solution.solve = orig
+    assert refhook._stop_rule(captured['cb'], mm, defaults) == (1e-7, 123.0)
