@@ -34,6 +34,7 @@ MMX_VARIANT_SHARED_STAGED = 2
 MMX_VARIANT_PERSISTENT = 4
 MMX_VARIANT_PLANE = 8
 MMX_VARIANT_FUSED_EPILOGUE = 16
+MMX_VARIANT_TMA = 32
 
 # numpy mirror of struct mmx_rhs_state (include/macromax_b200.h)
 STATE_DTYPE = np.dtype([

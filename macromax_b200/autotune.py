@@ -3,8 +3,8 @@ Autotuner for the kernel variant of an iteration plan.
 
 For one problem class -- (grid shape, components, chi kind, batch, precision, GPU) -- it times a few iterations of
 every kernel variant the plan offers (``mmx_plan_set_variant``: compile-time register-staged passes, shared-memory
-staged passes, the epilogue fused with the next prologue, persistent double-buffered prologue/epilogue, plane
-passes over the two inner axes of a 3D grid,
+staged passes, strided passes staged by bulk tensor (TMA) copies, the epilogue fused with the next prologue,
+persistent double-buffered prologue/epilogue, plane passes over the two inner axes of a 3D grid,
 runtime-length kernels) with CUDA events and keeps the
 fastest.  Results are cached in a JSON file (``$MACROMAX_B200_TUNE_CACHE`` or
 ``~/.cache/macromax_b200/autotune.json``), so a problem class is measured once per machine.  The trial iterations
@@ -21,8 +21,9 @@ import torch
 
 from . import _native as nat
 
-CANDIDATES = (0, nat.MMX_VARIANT_FUSED_EPILOGUE, nat.MMX_VARIANT_PLANE, nat.MMX_VARIANT_SHARED_STAGED,
-              nat.MMX_VARIANT_PERSISTENT,
+CANDIDATES = (0, nat.MMX_VARIANT_FUSED_EPILOGUE, nat.MMX_VARIANT_TMA,
+              nat.MMX_VARIANT_TMA | nat.MMX_VARIANT_FUSED_EPILOGUE, nat.MMX_VARIANT_PLANE,
+              nat.MMX_VARIANT_SHARED_STAGED, nat.MMX_VARIANT_PERSISTENT,
               nat.MMX_VARIANT_SHARED_STAGED | nat.MMX_VARIANT_PERSISTENT, nat.MMX_VARIANT_GENERIC)
 
 

@@ -7,6 +7,7 @@
 #include <string>
 #include <type_traits>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -16,6 +17,9 @@
 #include "mmx_epro.cuh"
 #include "mmx_magnetic.cuh"
 #include "mmx_fftr.cuh"
+#include "mmx_tma.cuh"
+
+#include <cudaTypedefs.h>
 
 #define MMX_ABI_VERSION 1
 
@@ -68,6 +72,21 @@ cudaError_t launch_pass(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sm
   return cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
+// Raise a kernel's dynamic shared-memory limit once per device.  `configured` is the calling launcher's own static
+// (one launcher per kernel instantiation) holding one bit per device ordinal; concurrent first calls may both set
+// the attribute, which is harmless.
+int allow_smem_once(std::atomic<uint64_t>& configured, const void* kern, int bytes) {
+  int dev = 0;
+  MMX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(MMX_ERR_ARG, "device ordinals above 63 are not supported");
+  const uint64_t bit = 1ull << dev;
+  if (!(configured.load(std::memory_order_acquire) & bit)) {
+    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    configured.fetch_or(bit, std::memory_order_release);
+  }
+  return MMX_OK;
+}
+
 struct PassCfg {
   int axis;
   int ops;
@@ -85,6 +104,8 @@ struct PassCfg {
   int regc_aniso = 0;  // 1: register-staged contiguous pass for a 3x3 chi (k_regc_aniso_pass), rc_tiles / rc_smem
   int64_t rc_tiles = 0;
   size_t rc_smem = 0;
+  int tma = 0;        // 1: strided pass staged by bulk tensor copies (k_tma_pass) through `tmap`
+  CUtensorMap tmap;   // 5-D map of the work buffer [B][C][outer][N][inner], box 16 x N x 1 x C x 1
 };
 
 bool reg_length(int n, int C) { return C == 3 ? (n == 64 || n == 128) : (n == 64 || n == 128 || n == 256 || n == 512); }
@@ -118,9 +139,13 @@ struct mmx_plan {
   bool force_generic = false;  // MMX_FORCE_GENERIC=1: use only the runtime-length kernels (tests)
   bool no_reg = false;         // MMX_NO_REG=1: shared-memory staged kernels for the strided passes (tests)
   bool pipe = false;           // MMX_PIPE=1: persistent double-buffered prologue/epilogue passes
+  // polls of k_pipe_pass's staged-input waits before it loads the tile from global memory instead and raises
+  // MMX_STATUS_TIMEOUT (MMX_PIPE_POLL_LIMIT, 0 .. 2^20: a test of that path; draining waits keep 2^20)
+  int poll_limit = 1 << 20;
   bool plane = false;          // plane passes over the two inner axes (3D, 128 x 128 planes, isotropic chi)
   std::vector<PassCfg> plane_passes;  // the 3-pass schedule used when `plane` is set and chi is isotropic
   bool epro = false;           // fuse each epilogue with the next iteration's prologue (isotropic chi)
+  bool tma = false;            // strided 128-sample passes staged by bulk tensor copies (k_tma_pass)
   std::vector<PassCfg> epro_passes;   // [middle passes..., EPI+PRO, repair]; the first PRO runs once per call
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
@@ -223,12 +248,10 @@ void choose_tile(const FFTAxis& ax, int C, int64_t outer, int64_t inner, int pre
 template <class R, int C, int CHI, int OPS>
 int launch_iter(const PassCfg& pc, IterArgs<R> a, int batch, cudaStream_t s) {
   auto kern = k_iter_pass<R, C, CHI, OPS>;
-  static int configured_mask = 0;  // per-device attribute set once (devices < 32)
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured_mask & (1 << dev))) {
-    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-    configured_mask |= (1 << dev);
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
   }
   a.outer = pc.outer;
   a.inner = pc.inner;
@@ -264,12 +287,10 @@ int dispatch_ops(const PassCfg& pc, const IterArgs<R>& a, int batch, cudaStream_
 template <int C, int CHI, int OPS, int N, bool STRIDED>
 int launch_fast(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
   auto kern = k_fast_pass<C, CHI, OPS, N, kFastP, STRIDED>;
-  static int configured_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured_mask & (1 << dev))) {
-    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-    configured_mask |= (1 << dev);
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
   }
   a.outer = pc.outer;
   a.inner = pc.inner;
@@ -305,12 +326,10 @@ int launch_reg(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) 
     return fail(MMX_ERR_ARG, "internal: no register-staged kernel for this length");
   } else {
     auto kern = k_reg_pass<C, OPS, N>;
-    static int configured_mask = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured_mask & (1 << dev))) {
-      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-        configured_mask |= (1 << dev);
+    static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+    {
+      const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+      if (rc_ != MMX_OK) return rc_;
     }
     a.outer = pc.outer;
     a.inner = pc.inner;
@@ -323,6 +342,37 @@ int launch_reg(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) 
   }
 }
 
+int sm_count();
+
+template <int C, int OPS, int N>
+int launch_tma(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  if constexpr (N != 128) {
+    return fail(MMX_ERR_ARG, "internal: no tensor-staged kernel for this length");
+  } else {
+    auto kern = k_tma_pass<C, OPS, N>;
+    const size_t smem = mmx_tma::Layout<C, N>::bytes();
+    static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+    {
+      const int rc_ = allow_smem_once(configured, (const void*)kern, (int)smem);
+      if (rc_ != MMX_OK) return rc_;
+    }
+    a.outer = pc.outer;
+    a.inner = pc.inner;
+    a.nrhs = batch;
+    const int64_t tiles_per_rhs = pc.outer * pc.inner / kRegP;
+    int per_sm = 1;  // resident CTAs per SM (two for the 3-component tiles; more for the scalar ones)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RegThreads<C, N>::value, smem) != cudaSuccess ||
+        per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 1;
+    }
+    const int64_t grid = std::min<int64_t>(tiles_per_rhs * batch, (int64_t)sm_count() * per_sm);
+    MMX_CUDA(launch_pass(kern, dim3((unsigned)grid), dim3(RegThreads<C, N>::value), smem, s, a, pc.tmap,
+                         (int)tiles_per_rhs));
+    return MMX_OK;
+  }
+}
+
 template <int C, int OPS, int N>
 int launch_regc(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
   if constexpr (N == 192 || N == 384 || (C == 3 && N > 128)) {
@@ -330,12 +380,10 @@ int launch_regc(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   } else {
     constexpr int PCK = (OPS & OP_EPI) ? RegCDefault<C, N>::PC_EPI : RegCDefault<C, N>::PC;
     auto kern = k_regc_pass<C, OPS, N, PCK>;
-    static int configured_mask = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured_mask & (1 << dev))) {
-      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-        configured_mask |= (1 << dev);
+    static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+    {
+      const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+      if (rc_ != MMX_OK) return rc_;
     }
     a.outer = pc.outer;
     a.inner = pc.inner;
@@ -350,12 +398,10 @@ template <int OPS, int N, int CHI>
 int launch_regc_aniso(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
   constexpr int PCK = RegCDefault<3, N>::PC;
   auto kern = k_regc_aniso_pass<OPS, N, PCK, CHI>;
-  static int configured_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured_mask & (1 << dev))) {
-    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-    configured_mask |= (1 << dev);
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
   }
   a.outer = pc.outer;
   a.inner = pc.inner;
@@ -365,13 +411,16 @@ int launch_regc_aniso(const PassCfg& pc, IterArgs<float> a, int batch, cudaStrea
   return MMX_OK;
 }
 
+// SM count of the current device, cached per device ordinal (0 .. 63)
 int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
+  static std::atomic<int> cached[64];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  int n = cached[dev].load(std::memory_order_relaxed);
+  if (n <= 0) {
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached[dev].store(n, std::memory_order_relaxed);
   }
   return n;
 }
@@ -384,12 +433,10 @@ int launch_pipe(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
     constexpr int PCK = RegCDefault<C, N>::PC_PIPE;
     auto kern = k_pipe_pass<C, OPS, N, PCK>;
     const size_t smem = PipeLayout<C, OPS, N, PCK>::bytes();
-    static int configured_mask = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured_mask & (1 << dev))) {
-      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-      configured_mask |= (1 << dev);
+    static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+    {
+      const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+      if (rc_ != MMX_OK) return rc_;
     }
     const int64_t tiles_per_rhs = pc.outer / PCK;
     const int64_t ntiles = tiles_per_rhs * batch;
@@ -408,12 +455,10 @@ template <int C, int OPS>
 int launch_plane(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
   auto kern = k_plane_pass<C, OPS>;
   const size_t smem = mmx_plane::smem_bytes();
-  static int configured_mask = 0;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(configured_mask & (1 << dev))) {
-    MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured_mask |= (1 << dev);
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)smem);
+    if (rc_ != MMX_OK) return rc_;
   }
   a.outer = pc.outer;
   a.inner = pc.inner;
@@ -430,12 +475,10 @@ int launch_epro(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   } else {
     constexpr int PCK = RegCDefault<C, N>::PC_EPI;
     auto kern = k_regc_epro<C, N, PCK>;
-    static int configured_mask = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured_mask & (1 << dev))) {
-      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-      configured_mask |= (1 << dev);
+    static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+    {
+      const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+      if (rc_ != MMX_OK) return rc_;
     }
     a.outer = pc.outer;
     a.inner = pc.inner;
@@ -455,21 +498,15 @@ int launch_repair(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t 
   } else {
     constexpr int PCK = RegCDefault<C, N>::PC;
     auto kern = k_regc_repair<C, N, PCK>;
-    static int configured_mask = 0;
-    static int blocks_per_sm = 1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured_mask & (1 << dev))) {
-      MMX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap));
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, RegC<C, N, PCK>::THREADS, pc.rc_smem);
-      if (blocks_per_sm < 1) blocks_per_sm = 1;
-      configured_mask |= (1 << dev);
+    static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+    {
+      const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+      if (rc_ != MMX_OK) return rc_;
     }
     a.outer = pc.outer;
     a.inner = pc.inner;
     a.nrhs = batch;
     // one CTA per SM: it only has work after a rejection, so the common, empty case should launch little
-    (void)blocks_per_sm;
     const int64_t grid = std::min<int64_t>(pc.rc_tiles, (int64_t)sm_count());
     MMX_CUDA(launch_pass(kern, dim3((unsigned)grid), dim3(RegC<C, N, PCK>::THREADS), pc.rc_smem, s, a,
                          (int)pc.rc_tiles));
@@ -516,6 +553,14 @@ int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_
       case OP_PRO | OP_FWD: return launch_regc<C, OP_PRO | OP_FWD, N>(pc, a, batch, s);
       case OP_INV | OP_EPI: return launch_regc<C, OP_INV | OP_EPI, N>(pc, a, batch, s);
       default: break;
+    }
+  }
+  if (pc.tma) {
+    switch (pc.ops) {
+      case OP_FWD: return launch_tma<C, OP_FWD, N>(pc, a, batch, s);
+      case OP_INV: return launch_tma<C, OP_INV, N>(pc, a, batch, s);
+      case OP_FWD | OP_G | OP_INV: return launch_tma<C, OP_FWD | OP_G | OP_INV, N>(pc, a, batch, s);
+      default: return fail(MMX_ERR_ARG, "internal: operation set without a tensor-staged kernel");
     }
   }
   if (pc.reg) {
@@ -571,6 +616,41 @@ int dispatch_pass(const PassCfg& pc, const IterArgs<R>& a, int C, int chi_kind, 
   if (chi_kind == MMX_CHI_SCALAR) return dispatch_ops<R, 3, MMX_CHI_SCALAR>(pc, a, batch, s);
   if (chi_kind == MMX_CHI_SYM6) return dispatch_ops<R, 3, MMX_CHI_SYM6>(pc, a, batch, s);
   return dispatch_ops<R, 3, MMX_CHI_MAT3>(pc, a, batch, s);
+}
+
+// cuTensorMapEncodeTiled from the driver (no link-time dependency on libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// The tile map of a strided pass over the plan's work buffer T [B][C][outer][n][inner] (complex64 words as 8-byte
+// elements): dimensions innermost first (inner, n, outer, C, B), box (16, n, 1, C, 1), the [c][j][pencil] tile of
+// k_tma_pass.  False when the geometry does not qualify (the pass then keeps k_reg_pass).
+bool encode_tile_map(const mmx_plan* p, int64_t outer, int n, int64_t inner, CUtensorMap* map) {
+  auto enc = tensor_map_encoder();
+  if (!enc || !p->work || inner % kRegP != 0 || n > 256 || p->ncomp > 256) return false;
+  const cuuint64_t dims[5] = {(cuuint64_t)inner, (cuuint64_t)n, (cuuint64_t)outer, (cuuint64_t)p->ncomp,
+                              (cuuint64_t)p->batch};
+  const cuuint64_t strides[4] = {(cuuint64_t)inner * 8, (cuuint64_t)n * inner * 8, (cuuint64_t)p->N * 8,
+                                 (cuuint64_t)p->ncomp * p->N * 8};
+  const cuuint32_t box[5] = {(cuuint32_t)kRegP, (cuuint32_t)n, 1u, (cuuint32_t)p->ncomp, 1u};
+  const cuuint32_t estr[5] = {1u, 1u, 1u, 1u, 1u};
+  for (int i = 0; i < 4; ++i)
+    if (strides[i] % 16 != 0) return false;
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, p->work, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
 }
 
 // pass sequence of one application of chi G chi (iteration) or of the FP64 defect
@@ -639,6 +719,7 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
         pc.sP = kRegP;
         pc.tiles = outer * inner / kRegP;
         pc.smem = ((size_t)p->ncomp * n * kRegP + n) * sizeof(float2);
+        if (p->tma && n == 128 && encode_tile_map(p, outer, n, inner, &pc.tmap)) pc.tma = 1;
       }
     }
     v.push_back(pc);
@@ -718,6 +799,7 @@ template <class R> IterArgs<R> base_args(mmx_plan* p) {
   a.done = p->done;
   a.l2_window = p->l2_persist ? p->l2_window : 0;
   a.inv_total = (R)(1.0 / (double)p->N);
+  a.poll_limit = p->poll_limit;
   return a;
 }
 
@@ -771,12 +853,10 @@ bool fftr_axis_n(const float2* in, float2* out, int64_t outer, int64_t inner, co
     if (inner % kRegP != 0 || scale != 1.0f) return false;
     const int64_t tiles = outer * inner / kRegP;
     const size_t smem = ((size_t)N * kRegP + N) * sizeof(float2);
-    static int configured_mask = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!(configured_mask & (1 << dev))) {  // 512-sample tiles need more than the default 48 KiB
-      cudaFuncSetAttribute(k_fftr_strided<DIR, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap);
-      configured_mask |= (1 << dev);
+    static std::atomic<uint64_t> configured{0};  // 512-sample tiles need more than the default 48 KiB
+    if (allow_smem_once(configured, (const void*)k_fftr_strided<DIR, N>, (int)kSmemCap) != MMX_OK) {
+      *err = cudaErrorInvalidValue;
+      return true;
     }
     k_fftr_strided<DIR, N><<<(unsigned)tiles, RegThreads<1, N>::value, smem, s>>>(in, out, inner, tw);
     *err = cudaGetLastError();
@@ -951,6 +1031,8 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
     p->no_reg = nr && nr[0] == '1';
     const char* pp = getenv("MMX_PIPE");
     p->pipe = pp && pp[0] == '1';
+    const char* pl = getenv("MMX_PIPE_POLL_LIMIT");
+    if (pl && pl[0]) p->poll_limit = std::max(0, std::min(1 << 20, atoi(pl)));
     const char* lp = getenv("MMX_L2_PERSIST");
     if (lp && lp[0] == '1' && precision == MMX_C64) {
       int maxp = 0, maxw = 0;
@@ -1230,13 +1312,14 @@ extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const 
 
 extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
   if (!p) return fail(MMX_ERR_ARG, "NULL plan");
-  if (flags & ~31u) return fail(MMX_ERR_ARG, "unknown variant flags");
+  if (flags & ~63u) return fail(MMX_ERR_ARG, "unknown variant flags");
   drop_graphs_of(p);  // captured graphs hold the previous kernels
   p->force_generic = (flags & MMX_VARIANT_GENERIC) != 0;
   p->no_reg = (flags & MMX_VARIANT_SHARED_STAGED) != 0;
   p->pipe = (flags & MMX_VARIANT_PERSISTENT) != 0;
   p->plane = (flags & MMX_VARIANT_PLANE) != 0;
   p->epro = (flags & MMX_VARIANT_FUSED_EPILOGUE) != 0;
+  p->tma = (flags & MMX_VARIANT_TMA) != 0;
   p->iter_passes = build_passes(p, false);
   p->defect_passes = build_passes(p, true);
   p->plane_passes = build_plane_passes(p);
@@ -1251,7 +1334,7 @@ extern "C" unsigned mmx_plan_get_variant(const mmx_plan* p) {
   if (!p) return 0u;
   return (p->force_generic ? MMX_VARIANT_GENERIC : 0u) | (p->no_reg ? MMX_VARIANT_SHARED_STAGED : 0u) |
          (p->pipe ? MMX_VARIANT_PERSISTENT : 0u) | (p->plane ? MMX_VARIANT_PLANE : 0u) |
-         (p->epro ? MMX_VARIANT_FUSED_EPILOGUE : 0u);
+         (p->epro ? MMX_VARIANT_FUSED_EPILOGUE : 0u) | (p->tma ? MMX_VARIANT_TMA : 0u);
 }
 
 extern "C" int mmx_mat3_extremes(mmx_plan* p, const void* M, int64_t nvox, int mode, double ab, double* out_dev,

@@ -45,6 +45,7 @@ template <class R> struct IterArgs {
   float2* aux;           // defect output [B][C][N] complex64
   size_t l2_window;      // bytes of T kept L2-resident (0: off); host-side launch attribute only
   int nrhs;              // number of right-hand sides (persistent passes)
+  int poll_limit;        // polls of a staged-input wait before the pass falls back to global loads (k_pipe_pass)
 };
 
 // Programmatic dependent launch.  The pass kernels are launched so that the next pass's CTAs may become resident

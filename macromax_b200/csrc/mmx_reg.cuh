@@ -430,10 +430,10 @@ template <int C, int N, int PC_> struct RegC {
   static __device__ __forceinline__ int idx(int c, int row, int m) { return (c * PC + row) * PITCH + m + (m >> 4); }
 };
 
-// bounded wait on an mbarrier phase; returns false if the copy did not complete within the limit
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// bounded wait on an mbarrier phase; returns false if the copy did not complete within `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit = 1 << 20) {
   const unsigned addr = (unsigned)__cvta_generic_to_shared(bar);
-  for (int it = 0; it < (1 << 20); ++it) {
+  for (int it = 0; it < limit; ++it) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, 1) k_pipe_pass(IterAr
       const int cur = s_cur[s];
       const float2* Ecur = cur ? a.E1 : a.E0;
       float2* Eoth = cur ? a.E0 : a.E1;
-      const bool staged = mbar_wait(&bars[s], parity);
+      const bool staged = mbar_wait(&bars[s], parity, a.poll_limit);
       if (!staged && tid == 0) atomicOr(&const_cast<mmx_rhs_state*>(st)->status, MMX_STATUS_TIMEOUT);
       const float2* stg = stage0 + s * L::STAGE;
       if constexpr ((OPS & OP_PRO) != 0) {

@@ -38,7 +38,9 @@ def _stream():
 
 class MixedSolution:
     def __init__(self, grid: Grid, sources, epsilon, bound=None, vacuum_wavelength=None, wavenumber=None,
-                 device=None):
+                 device=None, initial_field=None):
+        """``initial_field`` (optional, [B, C, *grid] or [C, *grid], in the units of ``E``): the FP64 iterate to start
+        from instead of zero, e.g. the solution of a nearby problem."""
         if not isinstance(grid, Grid):
             grid = Grid.from_ranges(*grid)
         self.grid = grid
@@ -77,6 +79,9 @@ class MixedSolution:
             self.src64 = torch.from_numpy(s_host).to(self.device).reshape(self.batch, self.ncomp, N)
             self.src64 *= 1.0j / pre.alpha.imag / pre.beta
             self.x = torch.zeros((self.batch, self.ncomp, N), dtype=torch.complex128, device=self.device)
+            if initial_field is not None:
+                x0 = torch.as_tensor(initial_field, dtype=torch.complex128, device=self.device)
+                self.x.copy_(torch.broadcast_to(x0.reshape(-1, self.ncomp, N), self.x.shape) * self.wavenumber ** 2)
             self._norms = torch.zeros(self.batch, dtype=torch.float64, device=self.device)
         self.outer_residues = []
         self.inner_iterations = []

@@ -29,6 +29,7 @@ def test_reference_arm_prints_the_contract_line():
     assert d['impl'] == 'reference' and d['n_gpus'] == 1 and d['steps'] == 2 and d['warmup'] == 3
     assert d['unit'] == 'voxel-it/s' and d['higher_is_better'] is True and d['value'] > 0
     assert d['config']['grid'] == [32, 32, 32] and d['config']['components'] == 3
+    assert d['config']['parallelism'] == 'replicas x1'  # the same config dict as the device arm's line
     assert d['cpu_baseline']['kind'] == 'port' and d['cpu_baseline']['value'] == d['value']
     assert d['e2e'] == {'value': d['value'], 'unit': d['unit'], 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}
 
@@ -44,3 +45,4 @@ def test_reference_arm_under_torchrun_prints_once():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _json_lines(r.stdout)
     assert len(lines) == 1 and lines[0]['impl'] == 'reference' and lines[0]['n_gpus'] == 2
+    assert lines[0]['config']['parallelism'] == 'replicas x2'

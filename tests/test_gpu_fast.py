@@ -158,3 +158,20 @@ def test_symmetric_chi_six_entries_equals_nine(dtype):
     a.solve(None, rtol=0, maxiter=20)
     b.solve(None, rtol=0, maxiter=20)
     assert rel(a.E, b.E) < (1e-6 if dtype == np.complex64 else 1e-13)
+
+
+def test_persistent_pipeline_wait_limit_raises_timeout_and_keeps_fields_exact():
+    """k_pipe_pass's staged-input wait gives up after MMX_PIPE_POLL_LIMIT polls (here 0, so every wait runs out): the
+    pass raises MMX_STATUS_TIMEOUT in the right-hand side's state, computes the tile from global memory instead and
+    drains its copies before re-arming the stage; the fields equal the single-tile passes' bit for bit."""
+    from macromax_b200 import _native as nat
+    wl = _cases()['spheres3d_64']()
+    pipe = _solution_env(wl, {'MMX_PIPE': '1', 'MMX_PIPE_POLL_LIMIT': '0'})
+    single = _solution_env(wl, {'MMX_PIPE': '0', 'MMX_PIPE_POLL_LIMIT': ''})
+    pipe.solve(None, rtol=0, maxiter=6)
+    single.solve(None, rtol=0, maxiter=6)
+    st = pipe._engine.read_state()
+    assert int(st['status'][0]) & nat.MMX_STATUS_TIMEOUT
+    assert int(single._engine.read_state()['status'][0]) == 0
+    assert pipe.iteration == single.iteration == 6
+    assert np.array_equal(pipe.E, single.E)

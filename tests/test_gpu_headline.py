@@ -94,3 +94,69 @@ def test_anisotropic_192_axis_matches_oracle(axis):
     for it in RECORD:
         assert rel(fields[it], ref[it]) < 1e-5, (axis, it, rel(fields[it], ref[it]))
 
+
+
+def _solve_variant(wl, variant, iters):
+    from macromax_b200 import Bound, Grid, Solution, autotune
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                   source_distribution=wl['source'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                   dtype=np.complex64)
+    autotune.set_variant(sol._engine, variant)
+    assert autotune.get_variant(sol._engine) == variant
+    sol.solve(None, rtol=0, maxiter=iters)
+    E, st = sol.E, sol._engine.read_state()
+    sol._engine.close()
+    return E, st
+
+
+@pytest.mark.parametrize('variant', [32, 48])
+def test_tensor_staged_passes_equal_register_staged_passes(spheres128, variant):
+    """The strided passes staged by bulk tensor copies (variant 32: k_tma_pass, alone and with the fused epilogue)
+    run the same arithmetic as k_reg_pass: identical fields, bit for bit, on the 128^3 vector workload; and the
+    oracle's iterates within 1e-5."""
+    wl, (alpha_ref, ref) = spheres128
+    a, st_a = _solve_variant(wl, variant, 20)
+    b, st_b = _solve_variant(wl, variant & ~32, 20)
+    assert int(st_a['status'][0]) == 0 and int(st_a['iteration'][0]) == 20
+    assert np.array_equal(a, b)
+    assert rel(a, ref[20]) < 1e-5
+
+
+def test_tensor_staged_scalar_passes_equal_register_staged_passes():
+    """The scalar (one-component) tensor-staged passes on the 128^3 design problem."""
+    from macromax_b200 import workloads
+    wl = workloads.design_3d(n=128)
+    a, st = _solve_variant(wl, 32, 12)
+    b, _ = _solve_variant(wl, 0, 12)
+    assert int(st['status'][0]) == 0
+    assert np.array_equal(a, b)
+
+
+def test_tensor_staged_passes_in_a_batch_with_finished_members():
+    """A batch whose members stop at different iterations: tiles of inactive right-hand sides are skipped without a
+    copy, and every member equals its solve with the register-staged passes."""
+    import torch
+    from macromax_b200 import Bound, Grid, autotune, workloads
+    from macromax_b200.batch import BatchSolution
+    wl = workloads.spheres_3d(n=128, nb_spheres=60)
+    src = np.stack([wl['source'], 0.3 * np.roll(wl['source'], 7, axis=2), np.roll(wl['source'], -5, axis=1)])
+    grid = Grid(shape=wl['shape'], step=wl['step'])
+    out = {}
+    for variant in (0, 32):
+        bs = BatchSolution(grid, src, wl['epsilon'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                           vacuum_wavelength=wl['wavelength'], dtype=np.complex64)
+        eng = bs.engine
+        autotune.set_variant(eng, variant)
+        st = eng.read_state()
+        st['iteration'], st['rtol'], st['active'], st['status'] = 0, -1.0, 1, 0
+        st['maxiter'] = [15, 30, 45]  # the members stop one after the other
+        eng.write_state(st)
+        for _ in range(6):
+            eng.iterate(8)
+        out[variant] = (bs.E.copy(), bs.iterations.copy())
+        bs.close()
+        torch.cuda.empty_cache()
+    assert list(out[32][1]) == [15, 30, 45]
+    assert np.array_equal(out[0][1], out[32][1])
+    assert np.array_equal(out[0][0], out[32][0])

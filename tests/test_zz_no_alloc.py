@@ -5,7 +5,8 @@ The allocation-free FFT entry point ``mmx_fftn_noalloc``, called through the C A
 ``mmx_fftn_noalloc`` serves callers that must not let a library allocate or free device memory -- applications
 whose buffers all come from their own pool or fixed memory plan, where a side cudaMalloc can fail on a fully
 committed GPU and a cudaFree stalls the device.  Its twiddle tables live in a file-scope device array shared by all
-calls, so the test also checks that a second call with another shape and precision does not see stale tables.
+calls, so the test also checks that a later call with another shape and precision does not see stale tables, up to
+the 4096-sample limit.
 This file is collected last (``test_zz``) so that a stop-at-first-failure run has finished every other test first.
 """
 import ctypes
@@ -48,7 +49,10 @@ TOL = {np.complex64: 2e-6, np.complex128: 1e-13}
 def test_noalloc_fft_matches_planned_fft_on_two_calls():
     import torch
     rng = np.random.default_rng(17)
-    calls = [((128, 96, 20), np.complex64, 0), ((30, 64), np.complex128, 1)]
+    # two ordinary calls, then the bound: a 4096-sample axis in the last twiddle slot (complex128, the largest
+    # words) and a 1-D 4096-sample transform
+    calls = [((128, 96, 20), np.complex64, 0), ((30, 64), np.complex128, 1), ((2, 3, 4096), np.complex128, 0),
+             ((4096,), np.complex64, 1)]
     for shape, dtype, inverse in calls:
         nb = 2
         x = (rng.standard_normal((nb, *shape)) + 1j * rng.standard_normal((nb, *shape))).astype(dtype)
