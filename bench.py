@@ -510,7 +510,11 @@ def run_secondary(args):
     b = time.perf_counter()
     S = np.asarray(sm)
     c = time.perf_counter()
-    out['scattering_matrix_slab2d_512x256'] = {'columns': int(S.shape[1]), 'setup_s': b - a, 'columns_s': c - b}
+    tm = getattr(sm, 'timing', {'modes_s': float('nan'), 'solve_s': float('nan')})
+    out['scattering_matrix_slab2d_512x256'] = {
+        'columns': int(S.shape[1]), 'setup_s': b - a, 'columns_s': c - b,
+        'solves_s': tm['solve_s'], 'mode_synthesis_and_detection_on_device_s': tm['modes_s'],
+        'other_host_s': (c - b) - tm['solve_s'] - tm['modes_s']}
     del S, sm
     # adjoint: one small untimed pass first, so that the first use of torch's autograd and indexing kernels (about
     # 1 s of one-time loading) is not counted in the timed forward / backward

@@ -61,7 +61,10 @@ typedef struct mmx_rhs_state {
   int32_t accepted;            /* 1 if the last update was accepted by the divergence guard */
   int32_t rejections;          /* number of rejected updates (alpha_i raised by 1.5x) */
   int32_t status;              /* MMX_STATUS_* */
-  int32_t reserved[2];
+  int32_t reserved[2];         /* [0]: used by mmx_magnetic_iterate.  [1]: bit c set = component c of this right-hand
+                                  side's source is identically zero, so the prologue may skip reading it; 0 claims
+                                  nothing.  Whoever writes the source clears or sets it (mmx_defect's output, for
+                                  instance, is a dense source: clear the bits of the states that read it). */
 } mmx_rhs_state;
 
 typedef struct mmx_plan mmx_plan;
@@ -267,6 +270,21 @@ int mmx_chi_from_eps(const void* eps, int m, int64_t nvox, double s_re, double s
  */
 int mmx_fftn_noalloc(int ndim, const int64_t* shape, const void* in, void* out, int64_t nbatch, int inverse,
                      int precision, void* stream);
+
+/*
+ * Scattering-matrix mode synthesis and detection (replaces the spectrum assignment of srcvec2freespace,
+ * matrix.py:528-610, and the spectrum lookup of detfield2detvec, matrix.py:685-755).  A row is one
+ * transverse plane of `row_len` complex words (precision MMX_C64 | MMX_C128); idx[nmodes] (device, int64) holds the
+ * spectrum position of every propagating mode.
+ *   mmx_mode_scatter: out[r][idx[m]] = coef[r][m] for r < nrows (the other words of `out` are left as they are);
+ *   mmx_mode_gather:  out[r][m] = in[r][idx[m]].
+ * conj = 1 conjugates each word on the way.  Positions outside [0, row_len) are skipped (scatter) or read as 0
+ * (gather).  The transverse transforms between them are mmx_fftn calls on a plan of the transverse shape.
+ */
+int mmx_mode_scatter(const void* coef, const int64_t* idx, int64_t nmodes, int64_t nrows, int64_t row_len, int conj,
+                     void* out, int precision, void* stream);
+int mmx_mode_gather(const void* in, const int64_t* idx, int64_t nmodes, int64_t nrows, int64_t row_len, int conj,
+                    void* out, int precision, void* stream);
 
 #ifdef __cplusplus
 }

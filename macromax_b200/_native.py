@@ -51,7 +51,7 @@ EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destro
             'mmx_pointwise_mul', 'mmx_fftn_noalloc', 'mmx_mat3_extremes', 'mmx_iterate_graph',
             'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant',
             'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby', 'mmx_chi_from_eps',
-            'mmx_magnetic_iterate']
+            'mmx_magnetic_iterate', 'mmx_mode_scatter', 'mmx_mode_gather']
 
 _lib = None
 

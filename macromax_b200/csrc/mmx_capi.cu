@@ -18,6 +18,7 @@
 #include "mmx_magnetic.cuh"
 #include "mmx_fftr.cuh"
 #include "mmx_tma.cuh"
+#include "mmx_modes.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -1655,4 +1656,46 @@ extern "C" int mmx_fftn_noalloc(int ndim, const int64_t* shape, const void* in, 
   cudaStream_t s = (cudaStream_t)stream;
   if (precision == MMX_C128) return fftn_noalloc<double>(desc, (unsigned char*)scratch, in, out, nbatch, inverse, s);
   return fftn_noalloc<float>(desc, (unsigned char*)scratch, in, out, nbatch, inverse, s);
+}
+
+// Scattering-matrix mode synthesis and detection (matrix.py:528-610, 685-755): scatter mode coefficients into rows of
+// transverse spectra, or gather them back.
+template <class R>
+int mode_copy(bool scatter, const void* in, const int64_t* idx, int64_t nmodes, int64_t nrows, int64_t row_len,
+              int conj, void* out, cudaStream_t s) {
+  const int64_t total = nrows * nmodes;
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>((total + threads - 1) / threads, (int64_t)sm_count() * 16);
+  if (scatter)
+    k_mode_scatter<R><<<(unsigned)blocks, threads, 0, s>>>((const cpx<R>*)in, idx, nmodes, nrows, row_len, conj,
+                                                          (cpx<R>*)out);
+  else
+    k_mode_gather<R><<<(unsigned)blocks, threads, 0, s>>>((const cpx<R>*)in, idx, nmodes, nrows, row_len, conj,
+                                                         (cpx<R>*)out);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+int mode_args_ok(const void* in, const int64_t* idx, int64_t nmodes, int64_t nrows, int64_t row_len, void* out,
+                 int precision) {
+  if (!in || !idx || !out) return fail(MMX_ERR_ARG, "NULL buffer or mode table");
+  if (nmodes < 0 || nrows < 0 || row_len < 1) return fail(MMX_ERR_ARG, "negative count or empty row");
+  if (precision != MMX_C64 && precision != MMX_C128) return fail(MMX_ERR_ARG, "precision must be MMX_C64 or MMX_C128");
+  return MMX_OK;
+}
+
+extern "C" int mmx_mode_scatter(const void* coef, const int64_t* idx, int64_t nmodes, int64_t nrows, int64_t row_len,
+                                int conj, void* out, int precision, void* stream) {
+  const int rc = mode_args_ok(coef, idx, nmodes, nrows, row_len, out, precision);
+  if (rc != MMX_OK || nmodes == 0 || nrows == 0) return rc;
+  if (precision == MMX_C128) return mode_copy<double>(true, coef, idx, nmodes, nrows, row_len, conj, out, (cudaStream_t)stream);
+  return mode_copy<float>(true, coef, idx, nmodes, nrows, row_len, conj, out, (cudaStream_t)stream);
+}
+
+extern "C" int mmx_mode_gather(const void* in, const int64_t* idx, int64_t nmodes, int64_t nrows, int64_t row_len,
+                               int conj, void* out, int precision, void* stream) {
+  const int rc = mode_args_ok(in, idx, nmodes, nrows, row_len, out, precision);
+  if (rc != MMX_OK || nmodes == 0 || nrows == 0) return rc;
+  if (precision == MMX_C128) return mode_copy<double>(false, in, idx, nmodes, nrows, row_len, conj, out, (cudaStream_t)stream);
+  return mode_copy<float>(false, in, idx, nmodes, nrows, row_len, conj, out, (cudaStream_t)stream);
 }

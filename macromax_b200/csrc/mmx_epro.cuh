@@ -81,6 +81,7 @@ __device__ __forceinline__ void regc_pro_tile(const IterArgs<float>& a, int b, i
   const float2* __restrict__ eS = Ecur + fbase + c * N3 + rowbase;
   const float2* __restrict__ sS = a.src + fbase + c * N3 + rowbase;
   const float2* __restrict__ xS = a.chi + rowbase;
+  const bool with_src = !source_is_zero(a.st + b, c);
 #pragma unroll 1
   for (int m = 0; m < NBT; ++m) {
     const int i = ii + m * TPP;
@@ -88,7 +89,8 @@ __device__ __forceinline__ void regc_pro_tile(const IterArgs<float>& a, int b, i
 #pragma unroll
     for (int q = 0; q < RAD; ++q) {
       const int s_ = i + q * T;
-      u[q] = (cc.a * xS[s_] + cc.b) * eS[s_] + cc.s * sS[s_];
+      u[q] = (cc.a * xS[s_] + cc.b) * eS[s_];
+      if (with_src) u[q] += cc.s * sS[s_];
     }
     bfly<float, RAD, -1>(u, smtw, N);
 #pragma unroll
@@ -140,7 +142,8 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, 
   if (threadIdx.x == 0) {  // inputs no kernel writes: chi and s'
     prefetch_l2(a.chi + row0, chunk);
 #pragma unroll
-    for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(a.src + ((int64_t)b * C + cc2) * N3 + row0, chunk);
+    for (int cc2 = 0; cc2 < C; ++cc2)
+      if (!source_is_zero(st, cc2)) prefetch_l2(a.src + ((int64_t)b * C + cc2) * N3 + row0, chunk);
   }
   pdl_wait();
   pdl_trigger();
@@ -192,6 +195,7 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, 
   const float2* __restrict__ sS = a.src + fbase + c * N3 + rowbase;
   const float2* __restrict__ xS = a.chi + rowbase;
   float2* __restrict__ eO = Eoth + fbase + c * N3 + rowbase;
+  const bool with_src = !source_is_zero(st, c);  // uniform over the component's warps
   double dd2 = 0.0, en2 = 0.0;
   float2 xf[NBL][RL];
 #pragma unroll
@@ -213,7 +217,8 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, 
       eO[s_] = en;
       dd2 += norm2d(d);
       en2 += norm2d(en);
-      xf[m][q] = x * en + cc.s * sS[s_];  // next iteration's chi(alpha) E' + s'(alpha), if E' is accepted
+      xf[m][q] = x * en;  // next iteration's chi(alpha) E' + s'(alpha), if E' is accepted
+      if (with_src) xf[m][q] += cc.s * sS[s_];
     }
     bfly<float, RL, -1>(xf[m], smtw, N);  // first forward stage of the reversed plan (span 1)
   }

@@ -67,6 +67,10 @@ template <class R> struct ChiCoef {
   R alpha_re, alpha_im;
 };
 
+// Component c of this right-hand side's normalised source is identically zero (bit c of reserved[1], set by the
+// caller that wrote the source; 0 claims nothing): the prologue may skip reading it.
+__device__ __forceinline__ bool source_is_zero(const mmx_rhs_state* st, int c) { return (st->reserved[1] >> c) & 1; }
+
 template <class R> __device__ __forceinline__ ChiCoef<R> chi_coef(const mmx_rhs_state* st) {
   // chi(alpha) = chi0 alpha0_i / alpha_i + i (alpha0 - alpha) / alpha_i ; s'(alpha) = s'0 alpha0_i / alpha_i
   const double ai = st->alpha_im, ar = st->alpha_re;

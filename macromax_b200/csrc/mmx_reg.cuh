@@ -578,7 +578,8 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
     prefetch_l2(a.chi + row0, chunk);
     if constexpr ((OPS & OP_PRO) != 0) {
 #pragma unroll
-      for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(a.src + ((int64_t)b * C + cc2) * a.N + row0, chunk);
+      for (int cc2 = 0; cc2 < C; ++cc2)
+        if (!source_is_zero(st, cc2)) prefetch_l2(a.src + ((int64_t)b * C + cc2) * a.N + row0, chunk);
     }
   }
   pdl_wait();
@@ -615,6 +616,7 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
     const float2* __restrict__ eS = Ecur + fbase + c * N3 + rowbase;
     const float2* __restrict__ sS = a.src + fbase + c * N3 + rowbase;
     const float2* __restrict__ xS = a.chi + rowbase;
+    const bool with_src = !source_is_zero(st, c);  // uniform over the component's warps
 #pragma unroll 1
     for (int m = 0; m < NBT; ++m) {
       const int i = ii + m * TPP;
@@ -622,7 +624,8 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
 #pragma unroll
       for (int q = 0; q < RAD; ++q) {
         const int s_ = i + q * T;
-        u[q] = (cc.a * xS[s_] + cc.b) * eS[s_] + cc.s * sS[s_];
+        u[q] = (cc.a * xS[s_] + cc.b) * eS[s_];
+        if (with_src) u[q] += cc.s * sS[s_];
       }
       bfly<float, RAD, -1>(u, smtw, N);
 #pragma unroll
@@ -785,7 +788,8 @@ __global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_pass
       for (int k = 0; k < M; ++k) m[k] = cc.a * xI[k * N3 + s_];
 #pragma unroll
       for (int r = 0; r < C; ++r) {
-        float2 acc = cc.b * e[r] + cc.s * sI[r * N3 + s_];
+        float2 acc = cc.b * e[r];
+        if (!source_is_zero(st, r)) acc += cc.s * sI[r * N3 + s_];
 #pragma unroll
         for (int s2 = 0; s2 < C; ++s2) acc += m[chi_entry<CHI>(r, s2)] * e[s2];
         u[r][q] = acc;

@@ -133,6 +133,18 @@ class IterationEngine:
             self.sources.copy_(t.reshape(-1, self.ncomp, self.N).expand(self.batch, self.ncomp, self.N))
         else:
             self.sources[index].copy_(t.reshape(self.ncomp, self.N))
+        self._mark_zero_sources()
+
+    def _mark_zero_sources(self):
+        """Record in every right-hand side's state which source components are identically zero (bit c of
+        reserved[1]); the prologue kernels then skip reading those components.  Whoever writes the sources by other
+        means clears the bits (the mixed-precision defect does)."""
+        zero = ~(self.sources != 0).any(dim=2)  # [B, C]
+        weights = torch.tensor([1 << c for c in range(self.ncomp)], dtype=torch.int32, device=self.device)
+        bits = (zero.to(torch.int32) * weights).sum(dim=1).cpu().numpy()
+        st = self.read_state()
+        st['reserved'][:, 1] = bits
+        self.write_state(st)
 
     # -- state ------------------------------------------------------------------------------------------------------
     def read_state(self) -> np.ndarray:

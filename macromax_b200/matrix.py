@@ -23,6 +23,9 @@ from __future__ import annotations
 
 from typing import Callable, Optional
 
+import ctypes
+import time
+
 import numpy as np
 import scipy.constants as const
 import torch
@@ -38,6 +41,17 @@ _DEFAULT_MAXITER = 10000
 
 def _default_callback(s) -> bool:
     return s.iteration < _DEFAULT_MAXITER and s.residue > _DEFAULT_RTOL
+
+
+def _stream():
+    s = torch.cuda.current_stream().cuda_stream
+    return ctypes.c_void_p(s) if s else None
+
+
+def _synced_time() -> float:
+    """Host time after the device has finished the queued work (phase timing of the batched columns)."""
+    torch.cuda.synchronize()
+    return time.perf_counter()
 
 
 def _unit(v: np.ndarray, axis: int = 0) -> np.ndarray:
@@ -180,18 +194,16 @@ class ScatteringMatrix:
         v = np.array(vector, dtype=self._dtype).reshape(2, self._modes.size, 1 + self._vectorial)
         return np.moveaxis(v, -1, 1)
 
-    def _freespace_planes(self, vectors: np.ndarray, planes) -> np.ndarray:
+    def _plane_coefficients(self, vectors: np.ndarray, planes):
         """
-        Free-space fields of the mode vectors ``vectors`` [B, 2, P, M] on the axis-0 planes ``planes``, as
-        [B, C, len(planes), *transverse] -- the planes of srcvec2freespace (matrix.py:528-610).
+        Spectral coefficients of the mode vectors ``vectors`` [B, 2, P, M] on the axis-0 planes ``planes``: for each
+        side (forward, backward) an array [B, C, len(planes), M] that goes to the transverse spectrum positions of the
+        modes, or None for a side without input.  The backward side's coefficients are conjugated here; its field is
+        the conjugate of their transform (srcvec2freespace, matrix.py:528-610).
         """
         grid = self._grid
         k0 = self._k0
         kdir = self._kdir
-        nb_pol = 1 + 2 * self._vectorial
-        B = vectors.shape[0]
-        shape_t = tuple(int(n) for n in grid.shape[1:])
-        nt = int(np.prod(shape_t)) if shape_t else 1
         x0 = np.ravel(grid[0])[list(planes)]
         first_t = np.asarray(grid.first[1:], dtype=float)
         vectors = vectors / np.sqrt(kdir[0])  # entrance-aperture compensation
@@ -200,10 +212,12 @@ class ScatteringMatrix:
             radial_dir = _unit(_dot0(kdir, axial) * kdir - axial)  # [3, M]
             radial_mode_dir = _unit(kdir[1:])                       # [2, M]
         origin_phase = np.exp(1j * k0 * _dot0(kdir[1:grid.ndim], first_t[:, None])) if grid.ndim > 1 else 1.0
-        out = np.zeros((B, nb_pol, len(planes), *shape_t), dtype=self._dtype)
+        prop = np.exp(1j * k0 * kdir[0][None, :] * x0[:, None])     # [planes, M]
+        out = []
         for side, direction in ((0, 1), (1, -1)):
             vs = vectors[:, side]  # [B, P, M]
             if not np.any(vs != 0):
+                out.append(None)
                 continue
             if direction < 0:
                 vs = vs.conj()
@@ -214,15 +228,64 @@ class ScatteringMatrix:
             else:
                 per_mode = vs                                                    # [B, 1, M]
             per_mode = per_mode * origin_phase
-            prop = np.exp(1j * k0 * kdir[0][None, :] * x0[:, None])             # [planes, M]
+            out.append((per_mode[:, :, None, :] * prop[None, None]).astype(self._dtype))
+        return out
+
+    def _freespace_planes(self, vectors: np.ndarray, planes) -> np.ndarray:
+        """
+        Free-space fields of the mode vectors ``vectors`` [B, 2, P, M] on the axis-0 planes ``planes``, as
+        [B, C, len(planes), *transverse] -- the planes of srcvec2freespace (matrix.py:528-610), on the host.
+        """
+        shape_t = tuple(int(n) for n in self._grid.shape[1:])
+        nt = int(np.prod(shape_t)) if shape_t else 1
+        B, nb_pol = vectors.shape[0], 1 + 2 * self._vectorial
+        out = np.zeros((B, nb_pol, len(planes), *shape_t), dtype=self._dtype)
+        for side, coef in enumerate(self._plane_coefficients(vectors, planes)):
+            if coef is None:
+                continue
             spec = np.zeros((B, nb_pol, len(planes), nt), dtype=self._dtype)
-            spec[..., self._modes[::-1]] = per_mode[:, :, None, :] * prop[None, None]
+            spec[..., self._modes[::-1]] = coef
             spec = spec.reshape(B, nb_pol, len(planes), *shape_t)
             field = np.fft.fftn(spec, axes=tuple(range(3, 3 + len(shape_t)))) if shape_t else spec
-            if direction < 0:
-                field = field.conj()
-            out += field
+            out += field.conj() if side == 1 else field
         return out
+
+    # -- the same on the device: spectra scattered / gathered by mmx_mode_scatter / mmx_mode_gather, transverse
+    # transforms by mmx_fftn (used by the batched columns of grids with transverse axes) ----------------------------
+    def _transverse(self) -> dict:
+        if getattr(self, '_transverse_state', None) is None:
+            from . import _native as nat
+            device = torch.device(self._device if self._device is not None else 'cuda')
+            shape_t = tuple(int(n) for n in self._grid.shape[1:])
+            prec = nat.MMX_C64 if self._dtype == np.complex64 else nat.MMX_C128
+            with torch.cuda.device(device):
+                plan = nat.Plan(shape_t, 1, 1, prec)
+            idx = torch.from_numpy(np.ascontiguousarray(self._modes[::-1], dtype=np.int64)).to(device)
+            self._transverse_state = dict(nat=nat, device=device, plan=plan, idx=idx, prec=prec, shape_t=shape_t,
+                                          nt=int(np.prod(shape_t)))
+        return self._transverse_state
+
+    def _freespace_planes_device(self, vectors: np.ndarray, planes) -> torch.Tensor:
+        """_freespace_planes on the device: [B, C, len(planes), *transverse] (only the mode coefficients cross the
+        host link)."""
+        ts = self._transverse()
+        nat, idx, nt = ts['nat'], ts['idx'], ts['nt']
+        B, nb_pol, npl = vectors.shape[0], 1 + 2 * self._vectorial, len(planes)
+        rows = B * nb_pol * npl
+        tdtype = torch.complex64 if self._dtype == np.complex64 else torch.complex128
+        out = torch.zeros((rows, nt), dtype=tdtype, device=ts['device'])
+        stream = _stream()
+        for side, coef in enumerate(self._plane_coefficients(vectors, planes)):
+            if coef is None:
+                continue
+            c_dev = torch.from_numpy(np.ascontiguousarray(coef)).to(ts['device'])
+            spec = torch.zeros((rows, nt), dtype=tdtype, device=ts['device'])
+            nat.call('mmx_mode_scatter', nat.device_ptr(c_dev), nat.device_ptr(idx), int(idx.numel()), rows, nt, 0,
+                     nat.device_ptr(spec), ts['prec'], stream)
+            field = torch.empty_like(spec)
+            nat.call('mmx_fftn', ts['plan'].handle, nat.device_ptr(spec), nat.device_ptr(field), rows, 0, stream)
+            out += field.conj() if side == 1 else field
+        return out.reshape(B, nb_pol, npl, *ts['shape_t'])
 
     def srcvec2freespace(self, input_vector) -> np.ndarray:
         """Superposition of the vector's free-space plane waves on the whole grid (matrix.py:528-610)."""
@@ -260,12 +323,21 @@ class ScatteringMatrix:
         return np.stack(out, axis=2)
 
     def _device_sources(self, vectors: np.ndarray) -> torch.Tensor:
-        """_sources built on the device from the two source planes: only [B, C, 2, *transverse] crosses the host link
-        and no dense host array of the batch's size is made."""
-        device = torch.device(self._device if self._device is not None else 'cuda')
-        planes = torch.from_numpy(np.ascontiguousarray(self._source_plane_fields(vectors))).to(device)
+        """_sources built on the device: each source plane synthesised there (mmx_mode_scatter + mmx_fftn), so only
+        the mode coefficients cross the host link and no dense host array of the batch's size is made."""
+        scaled = vectors * self._source_scale()
+        if self._grid.ndim > 1:
+            planes = []
+            for side in range(2):
+                masked = np.zeros_like(scaled)
+                masked[:, side] = scaled[:, side]
+                planes.append(self._freespace_planes_device(masked, [self._source_planes[side]])[:, :, 0])
+            planes = torch.stack(planes, dim=2)
+        else:
+            device = torch.device(self._device if self._device is not None else 'cuda')
+            planes = torch.from_numpy(np.ascontiguousarray(self._source_plane_fields(vectors))).to(device)
         B, C = planes.shape[:2]
-        src = torch.zeros((B, C, *(int(n) for n in self._grid.shape)), dtype=planes.dtype, device=device)
+        src = torch.zeros((B, C, *(int(n) for n in self._grid.shape)), dtype=planes.dtype, device=planes.device)
         for side in range(2):  # in _sources' order: a shared plane keeps the front side's field
             src[:, :, self._source_planes[side]] = planes[:, :, side]
         return src
@@ -296,18 +368,41 @@ class ScatteringMatrix:
     def _detect(self, det_fields: np.ndarray) -> np.ndarray:
         """
         Detection vectors [B, side x mode x polarisation] from the outward fields on the detection planes,
-        det_fields [B, C, 2 (back plane, front plane), *transverse] (detfield2detvec, matrix.py:685-755).
+        det_fields [B, C, 2 (back plane, front plane), *transverse] (detfield2detvec, matrix.py:685-755), on the host.
         """
-        grid = self._grid
-        k0 = self._k0
-        kdir = self._kdir[:, None, :]  # [3, 1, M]
         B, nb_pol = det_fields.shape[:2]
-        shape_t = tuple(int(n) for n in grid.shape[1:])
+        shape_t = tuple(int(n) for n in self._grid.shape[1:])
         f = det_fields.astype(self._dtype, copy=True)
         f[:, :, 1] = f[:, :, 1].conj()  # the backward-propagating side
         if shape_t:
             f = np.fft.ifftn(f, axes=tuple(range(3, 3 + len(shape_t))))
-        at_modes = f.reshape(B, nb_pol, 2, -1)[..., self._modes[::-1]]  # [B, C, 2, M]
+        return self._mode_vectors(f.reshape(B, nb_pol, 2, -1)[..., self._modes[::-1]])
+
+    def _detect_device(self, det_fields: torch.Tensor) -> np.ndarray:
+        """_detect for device fields [B, C, 2, *transverse]: the conjugation, the inverse transverse transform and the
+        gather at the mode positions on the device (mmx_fftn, mmx_mode_gather); the mode amplitudes go to the host."""
+        ts = self._transverse()
+        nat, idx, nt = ts['nat'], ts['idx'], ts['nt']
+        B, nb_pol = det_fields.shape[:2]
+        rows = B * nb_pol * 2
+        f = det_fields.reshape(B, nb_pol, 2, nt).clone()
+        f[:, :, 1] = f[:, :, 1].conj()  # the backward-propagating side
+        f = f.reshape(rows, nt)
+        spec = torch.empty_like(f)
+        stream = _stream()
+        nat.call('mmx_fftn', ts['plan'].handle, nat.device_ptr(f), nat.device_ptr(spec), rows, 1, stream)
+        at = torch.empty((rows, int(idx.numel())), dtype=f.dtype, device=f.device)
+        nat.call('mmx_mode_gather', nat.device_ptr(spec), nat.device_ptr(idx), int(idx.numel()), rows, nt, 0,
+                 nat.device_ptr(at), ts['prec'], stream)
+        return self._mode_vectors(at.cpu().numpy().reshape(B, nb_pol, 2, -1))
+
+    def _mode_vectors(self, at_modes: np.ndarray) -> np.ndarray:
+        """Detection vectors from the complex amplitudes of the modes on the two detection planes, [B, C, 2, M]: the
+        polarisation basis, the phases to the grid origin and to the detection planes, and the aperture weight."""
+        grid = self._grid
+        k0 = self._k0
+        kdir = self._kdir[:, None, :]  # [3, 1, M]
+        B = at_modes.shape[0]
         if self._vectorial:
             k3 = kdir[:, 0, :]                                                          # [3, M]
             at_modes = at_modes - np.einsum('bism,im->bsm', at_modes, k3)[:, None] * k3[None, :, None, :]
@@ -327,7 +422,7 @@ class ScatteringMatrix:
         vec = vec * np.sqrt(kdir[0])
         vec = np.moveaxis(vec, 1, -1)  # [B, 2, M, P]
         vec[:, 1] = vec[:, 1].conj()
-        return vec.reshape(B, -1)
+        return vec.reshape(B, -1).astype(self._dtype, copy=False)
 
     def detfield2detvec(self, field) -> np.ndarray:
         """Detection vector of an outward field given on the whole grid (matrix.py:685-755)."""
@@ -341,36 +436,55 @@ class ScatteringMatrix:
 
     # -- columns: batched solves on the device ----------------------------------------------------------------------
     def _batched_outward(self, vectors: np.ndarray) -> np.ndarray:
-        """Detection vectors of the mode vectors [B, 2, P, M], all solved in batched launches."""
+        """Detection vectors of the mode vectors [B, 2, P, M], all solved in batched launches.  With transverse axes
+        the mode synthesis (sources, incident fields) and the detection run on the device; ``self.timing`` keeps the
+        seconds spent in them and in the solves."""
         nb_pol = 1 + 2 * self._vectorial
         B = vectors.shape[0]
         out = np.empty((B, self._side), dtype=self._dtype)
         word = np.dtype(self._dtype).itemsize
         per_rhs = 5.0 * nb_pol * self._grid.size * word  # two field buffers, work buffer, sources, staging
         chunk = int(max(1, min(self._max_batch, self._max_batch_bytes // per_rhs)))
-        # incident fields on the detection planes: the back detector sees the back input, the front detector the
-        # front input (matrix.py:795-800)
-        incident = np.zeros((B, nb_pol, 2, *self._grid.shape[1:]), dtype=self._dtype)
-        for plane_idx, side in ((0, 1), (1, 0)):
-            masked = np.zeros_like(vectors)
-            masked[:, side] = vectors[:, side]
-            incident[:, :, plane_idx] = self._freespace_planes(masked, [self._detector_planes[plane_idx]])[:, :, 0]
+        on_device = self._grid.ndim > 1
+        timing = self.__dict__.setdefault('timing', {'modes_s': 0.0, 'solve_s': 0.0})
+
+        def incident_fields(vec):
+            """Incident fields on the detection planes: the back detector sees the back input, the front detector
+            the front input (matrix.py:795-800)."""
+            planes = []
+            for plane_idx, side in ((0, 1), (1, 0)):
+                masked = np.zeros_like(vec)
+                masked[:, side] = vec[:, side]
+                plane = [self._detector_planes[plane_idx]]
+                planes.append(self._freespace_planes_device(masked, plane)[:, :, 0] if on_device
+                              else self._freespace_planes(masked, plane)[:, :, 0])
+            return torch.stack(planes, dim=2) if on_device else np.stack(planes, axis=2)
+
         pre = self._solution._pre
         bound = self._solution.bound
         k0 = self._k0
         rtol, maxiter = _DEFAULT_RTOL, _DEFAULT_MAXITER
         for b0 in range(0, B, chunk):
             sl = slice(b0, min(B, b0 + chunk))
+            t0 = _synced_time()
             src = self._device_sources(vectors[sl])
+            incident = incident_fields(vectors[sl])
+            t1 = _synced_time()
             bs = BatchSolution(self._grid, src, None, bound=bound, wavenumber=k0, dtype=self._dtype,
                                device=self._device, preconditioner=pre)
             del src
             bs.solve(rtol=rtol, maxiter=maxiter)
             E = bs.E_device.reshape(bs.batch, nb_pol, *(int(n) for n in self._grid.shape))
-            det = torch.stack([E[:, :, p] for p in self._detector_planes], dim=2)
-            det = det.cpu().numpy().astype(self._dtype) / (k0 ** 2)
+            det = torch.stack([E[:, :, p] for p in self._detector_planes], dim=2) * (1.0 / k0 ** 2)
             bs.close()
-            out[sl] = self._detect(det - incident[sl])
+            t2 = _synced_time()
+            if on_device:
+                out[sl] = self._detect_device((det.to(incident.dtype) - incident).contiguous())
+            else:
+                out[sl] = self._detect(det.cpu().numpy().astype(self._dtype) - incident)
+            t3 = _synced_time()
+            timing['modes_s'] += (t1 - t0) + (t3 - t2)
+            timing['solve_s'] += t2 - t1
         return out
 
     def _matvec_columns(self, right: np.ndarray) -> np.ndarray:

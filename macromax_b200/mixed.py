@@ -109,6 +109,7 @@ class MixedSolution:
         st['maxiter'] = 1
         st['active'] = (~done).astype(np.int32)
         st['status'] = 0
+        st['reserved'][:, 1] = 0  # the defect overwrites the inner sources: no component is known to be zero
         eng.write_state(st)
         nat.call('mmx_defect', self.plan64.handle, _ptr(self.x), _ptr(self.chi64), self.chi64_kind, _ptr(self.src64),
                  _ptr(eng.state), _ptr(eng.sources), _stream())

@@ -160,3 +160,29 @@ def test_tensor_staged_passes_in_a_batch_with_finished_members():
     assert list(out[32][1]) == [15, 30, 45]
     assert np.array_equal(out[0][1], out[32][1])
     assert np.array_equal(out[0][0], out[32][0])
+
+
+@pytest.mark.parametrize('variant', [0, 16])
+def test_zero_source_components_are_skipped_without_changing_the_iterates(spheres128, variant):
+    """The headline source is x-polarised, so components 1 and 2 of s' are identically zero: set_sources marks them
+    (bit c of the state's reserved[1]) and the prologue kernels skip reading them.  The iterates equal those of the
+    same solve with the marks cleared (every component read)."""
+    from macromax_b200 import Bound, Grid, Solution, autotune
+    wl = spheres128[0]
+    fields = []
+    for keep in (True, False):
+        grid = Grid(shape=wl['shape'], step=wl['step'])
+        sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                       source_distribution=wl['source'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                       dtype=np.complex64)
+        eng = sol._engine
+        autotune.set_variant(eng, variant)
+        st = eng.read_state()
+        assert int(st['reserved'][0, 1]) == 0b110
+        if not keep:
+            st['reserved'][:, 1] = 0
+            eng.write_state(st)
+        sol.solve(None, rtol=0, maxiter=12)
+        fields.append(sol.E)
+        eng.close()
+    assert np.array_equal(fields[0], fields[1])

@@ -51,3 +51,32 @@ def test_lossless_slab_is_nearly_unitary():
     S = np.asarray(make(z))
     sv = np.linalg.svd(S, compute_uv=False)
     assert np.allclose(sv, 1.0, atol=2e-2)
+
+
+@pytest.mark.parametrize('vectorial, dtype, tol', [(False, np.complex128, 1e-12), (True, np.complex128, 1e-12),
+                                                   (True, np.complex64, 2e-6)])
+def test_device_mode_synthesis_and_detection_equal_host(vectorial, dtype, tol):
+    """The batched columns synthesise their sources and incident fields and detect the outward fields on the device
+    (mmx_mode_scatter / mmx_mode_gather around mmx_fftn over the transverse planes); both equal the host
+    restatements of srcvec2freespace (matrix.py:528-610) and detfield2detvec (matrix.py:685-755) on random mode
+    vectors and fields of a 3D grid (2-D transverse planes)."""
+    import torch
+    from macromax_b200 import Grid
+    from macromax_b200.matrix import ScatteringMatrix
+    wavelength = 500e-9
+    grid = Grid(shape=(24, 20, 16), step=wavelength / 4)
+    sm = ScatteringMatrix(grid, vectorial=vectorial, vacuum_wavelength=wavelength, epsilon=1.0, dtype=dtype)
+    rng = np.random.default_rng(3)
+    B, P, M = 5, 1 + vectorial, sm._modes.size
+    assert M > 10
+    vectors = (rng.standard_normal((B, 2, P, M)) + 1j * rng.standard_normal((B, 2, P, M))).astype(dtype)
+    vectors[1, 1] = 0  # a side without input
+    planes = [3, 11, 20]
+    host = sm._freespace_planes(vectors, planes)
+    dev = sm._freespace_planes_device(vectors, planes).cpu().numpy()
+    assert rel(dev, host) < tol
+    C = 1 + 2 * vectorial
+    det = (rng.standard_normal((B, C, 2, 20, 16)) + 1j * rng.standard_normal((B, C, 2, 20, 16))).astype(dtype)
+    a = sm._detect(det)
+    b = sm._detect_device(torch.from_numpy(det).cuda())
+    assert rel(b, a) < tol
