@@ -48,7 +48,7 @@ class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
     QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
-             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,clocks.mem')
 
     def __init__(self, index: int):
         self.index = index
@@ -93,8 +93,10 @@ class ClockSampler:
             for i, nme in enumerate(names):
                 if len(s) > 5 + i and s[5 + i].lower().startswith('active'):
                     reasons.add(nme)
+        mem = [float(s[9]) for s in self.samples if len(s) > 9 and s[9].replace('.', '').isdigit()]
         return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': max(smax) if smax else None,
-                'reasons': sorted(reasons), 'samples': len(self.samples)}
+                'reasons': sorted(reasons), 'samples': len(self.samples),
+                'mem_mhz': statistics.median(mem) if mem else None}
 
 
 def make_workload(args):
@@ -310,7 +312,8 @@ def run_secondary(args):
         of 8 seeded sources against FP64 solutions, against the plain complex64 per-source loop (one Solution per
         source for all 256 sources, to 1e-5: single precision cannot reach 1e-8); and the uneven batch
         64 x 128^2 + 32 x 256^2 + 8 x 384^2 to 1e-8;
-      - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve to 1e-6.
+      - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve in complex64 to 1e-6,
+        and in mixed precision to 1e-10, each gradient's error against the same gradient from FP64 solves.
     """
     import torch
     from macromax_b200 import Bound, Grid, Solution, adjoint, workloads
@@ -553,6 +556,28 @@ def run_secondary(args):
         'solve_s (forward + adjoint iterations only)': solve_s,
         'solve_voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / solve_s,
         'gradient_error_vs_fp64_adjoint': adjoint_fp64_error(wl, g32)}
+    del g32
+    torch.cuda.empty_cache()
+    # the same gradient with both solves in mixed precision (complex64 inner iterations, FP64 defect correction to
+    # residue 1e-10): accurate beyond what complex64 solves reach
+    eps = torch.tensor(wl['epsilon'], dtype=torch.complex64, device='cuda', requires_grad=True)
+    src = torch.tensor(wl['source'], dtype=torch.complex64, device='cuda')
+    stats = {}
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    E = adjoint.solve(eps, src, grid, k0, bound=Bound(grid, thickness=wl['bound_thickness']), rtol=1e-10,
+                      stats=stats, precision='mixed')
+    loss = -(E[:, 0][(slice(None),) + wl['patch']].abs() ** 2).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    gm = eps.grad.detach().to(torch.complex128).cpu().numpy()
+    del E, loss, eps, src
+    torch.cuda.empty_cache()
+    out['adjoint_design3d_128x32']['mixed_precision'] = {
+        'forward_and_backward_s': b - a, 'forward_inner_iterations': int(stats['forward_iterations'][0]),
+        'adjoint_inner_iterations': int(stats['adjoint_iterations'][0]),
+        'gradient_error_vs_fp64_adjoint': adjoint_fp64_error(wl, gm)}
     return out
 
 

@@ -112,6 +112,8 @@ def load(path: str | None = None):
         'mmx_mat3_extremes': (i32, [vp, vp, i64, i32, dbl, vp, vp]),
         'mmx_iterate_graph': (i32, [vp, vp, vp, vp, i32, vp, vp, i32, vp]),
         'mmx_iterate_graph_prepare': (i32, [vp, vp, vp, vp, i32, vp, vp, i32]),
+        'mmx_mode_scatter': (i32, [vp, vp, i64, i64, i64, i32, vp, i32, vp]),
+        'mmx_mode_gather': (i32, [vp, vp, i64, i64, i64, i32, vp, i32, vp]),
         'mmx_plan_set_variant': (i32, [vp, ctypes.c_uint]),
         'mmx_plan_get_variant': (ctypes.c_uint, [vp]),
         'mmx_iterate_multi': (i32, [i32, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),

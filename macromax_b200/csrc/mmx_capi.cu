@@ -19,6 +19,7 @@
 #include "mmx_fftr.cuh"
 #include "mmx_tma.cuh"
 #include "mmx_modes.cuh"
+#include "mmx_magpass.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -1441,6 +1442,126 @@ extern "C" int mmx_axpby(void* out, const void* x, const void* y, double a_re, d
 }
 
 namespace {
+// ---- fused pass schedule for magnetic media (mmx_magpass.cuh), 2D and 3D grids ----
+struct MagPass {
+  int mode;
+  int axis;
+  PassCfg pc;
+};
+
+std::vector<MagPass> build_mag_passes(const mmx_plan* p) {
+  std::vector<MagPass> v;
+  const int d = p->ndim;
+  if (d < 2 || d > 3) return v;
+  auto add = [&](int mode, int axis, int C) {
+    MagPass mp;
+    mp.mode = mode;
+    mp.axis = axis;
+    int64_t outer = 1, inner = 1;
+    for (int i = 0; i < axis; ++i) outer *= p->shape[i];
+    for (int i = axis + 1; i < d; ++i) inner *= p->shape[i];
+    // small grids (the reference's 2D magnetic cases) have few pencils: ask for at least two tiles per SM
+    choose_tile(p->ax[axis], C, outer, inner, p->prec, mp.pc, 2 * (int64_t)sm_count());
+    mp.pc.axis = axis;
+    v.push_back(mp);
+  };
+  const int last = d - 1;
+  add(MAG_E_FWD, last, 3);
+  if (d == 3) add(MAG_MID_FWD3, 1, 3);
+  add(MAG_K_CURL_E, 0, 3);
+  if (d == 3) add(MAG_MID_INV3, 1, 3);
+  add(MAG_MIX1, last, 6);
+  if (d == 3) add(MAG_MID_FWD6, 1, 6);
+  add(MAG_K_GREEN, 0, 6);
+  if (d == 3) add(MAG_MID_INV6, 1, 6);
+  add(MAG_MIX2, last, 6);
+  if (d == 3) add(MAG_MID_FWD3, 1, 3);
+  add(MAG_K_CURL, 0, 3);
+  if (d == 3) add(MAG_MID_INV3, 1, 3);
+  add(MAG_UPDATE, last, 3);
+  for (const MagPass& mp : v)
+    if (2 * mp.pc.tiles > p->partials_len || mp.pc.smem > kSmemCap) return std::vector<MagPass>();
+  return v;
+}
+
+template <class R, int MODE>
+int launch_mag(const PassCfg& pc, MagArgs<R> a, cudaStream_t s) {
+  auto kern = k_mag_pass<R, MODE>;
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  a.P = pc.P;
+  a.sP = pc.sP;
+  kern<<<(unsigned)pc.tiles, pc.threads, pc.smem, s>>>(a);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
+template <class R>
+int dispatch_mag(const MagPass& mp, const MagArgs<R>& a, cudaStream_t s) {
+  switch (mp.mode) {
+    case MAG_E_FWD: return launch_mag<R, MAG_E_FWD>(mp.pc, a, s);
+    case MAG_MID_FWD3: return launch_mag<R, MAG_MID_FWD3>(mp.pc, a, s);
+    case MAG_MID_INV3: return launch_mag<R, MAG_MID_INV3>(mp.pc, a, s);
+    case MAG_MID_FWD6: return launch_mag<R, MAG_MID_FWD6>(mp.pc, a, s);
+    case MAG_MID_INV6: return launch_mag<R, MAG_MID_INV6>(mp.pc, a, s);
+    case MAG_K_CURL_E: return launch_mag<R, MAG_K_CURL_E>(mp.pc, a, s);
+    case MAG_K_GREEN: return launch_mag<R, MAG_K_GREEN>(mp.pc, a, s);
+    case MAG_K_CURL: return launch_mag<R, MAG_K_CURL>(mp.pc, a, s);
+    case MAG_MIX1: return launch_mag<R, MAG_MIX1>(mp.pc, a, s);
+    case MAG_MIX2: return launch_mag<R, MAG_MIX2>(mp.pc, a, s);
+    case MAG_UPDATE: return launch_mag<R, MAG_UPDATE>(mp.pc, a, s);
+    default: return fail(MMX_ERR_ARG, "internal: unknown magnetic pass");
+  }
+}
+
+// niter iterations on the fused schedule; work[0..4] hold A, B, U2, FFT(E) and the second field buffer.  The field
+// is settled back into b->E (and cur to 0) at the end of the chunk.
+template <class R>
+int run_magnetic_fused(mmx_plan* p, const std::vector<MagPass>& passes, const mmx_magnetic_buffers* b,
+                       mmx_rhs_state* st, int niter, cudaStream_t s) {
+  using C = cpx<R>;
+  MagArgs<R> a;
+  memset(&a, 0, sizeof(a));
+  a.N = p->N;
+  a.ndim = p->ndim;
+  for (int i = 0; i < 3; ++i) {
+    a.dims[i] = (int)p->shape[i];
+    a.kv[i] = p->kv_dev ? (const R*)p->kv_dev + p->kv_off[i] : nullptr;
+  }
+  a.inv_total = (R)(1.0 / (double)p->N);
+  a.E0 = (C*)b->E;
+  a.E1 = (C*)b->work[4];
+  a.src = (const C*)b->src;
+  a.ee = (const C*)b->chi_ee;
+  a.eh = (const C*)b->chi_eh;
+  a.he = (const C*)b->chi_he;
+  a.hh = (const C*)b->chi_hh;
+  a.A = (C*)b->work[0];
+  a.B = (C*)b->work[1];
+  a.U2 = (C*)b->work[2];
+  a.Eh = (C*)b->work[3];
+  a.st = st;
+  a.partials = p->partials;
+  a.done = p->done;
+  for (int it = 0; it < niter; ++it) {
+    for (const MagPass& mp : passes) {
+      a.ax = p->ax[mp.axis];
+      const int rc = dispatch_mag<R>(mp, a, s);
+      if (rc != MMX_OK) return rc;
+    }
+  }
+  const int64_t n3 = 3 * p->N;
+  k_mag_settle<R><<<grid_blocks(n3, 256), 256, 0, s>>>(a.E0, a.E1, st, n3);
+  k_mag_settle_state<<<1, 32, 0, s>>>(st);
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
 // niter iterations of the magnetic split-Richardson iteration with the decisions on the device (mmx_magnetic.cuh)
 template <class R>
 int run_magnetic(mmx_plan* p, const mmx_magnetic_buffers* b, mmx_rhs_state* st, int niter, cudaStream_t s) {
@@ -1504,12 +1625,22 @@ extern "C" int mmx_magnetic_iterate(mmx_plan* p, const mmx_magnetic_buffers* b, 
   if (p->batch != 1 || p->ncomp != 1) return fail(MMX_ERR_ARG, "the plan must be a 1-component, 1-batch plan");
   if (niter < 1) return fail(MMX_ERR_ARG, "niter must be positive");
   cudaStream_t s = (cudaStream_t)stream;
-  if (!use_graph)
-    return p->prec == MMX_C128 ? run_magnetic<double>(p, b, st, niter, s) : run_magnetic<float>(p, b, st, niter, s);
+  // the composition of eight batched transforms (the faster one on the measured grids) unless MMX_MAG_FUSED=1 asks
+  // for the fused pass schedule (2D and 3D grids)
+  const char* fused_env = getenv("MMX_MAG_FUSED");
+  const bool want_fused = fused_env && fused_env[0] == '1';
+  const std::vector<MagPass> fused = want_fused ? build_mag_passes(p) : std::vector<MagPass>();
+  auto run = [&](cudaStream_t cs) {
+    if (!fused.empty())
+      return p->prec == MMX_C128 ? run_magnetic_fused<double>(p, fused, b, st, niter, cs)
+                                 : run_magnetic_fused<float>(p, fused, b, st, niter, cs);
+    return p->prec == MMX_C128 ? run_magnetic<double>(p, b, st, niter, cs) : run_magnetic<float>(p, b, st, niter, cs);
+  };
+  if (!use_graph) return run(s);
   GraphKey key;
   key.ptrs = {(const void*)p, b->E, b->src, b->chi_ee, b->chi_eh, b->chi_he, b->chi_hh, (const void*)st};
   for (int i = 0; i < 7; ++i) key.ptrs.push_back(b->work[i]);
-  key.ints = {-3, niter};  // -3: a magnetic iteration chunk
+  key.ints = {fused.empty() ? -3 : -4, niter};  // a magnetic iteration chunk (-4: the fused schedule)
   cudaGraphExec_t exec = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_graph_mutex);
@@ -1523,7 +1654,7 @@ extern "C" int mmx_magnetic_iterate(mmx_plan* p, const mmx_magnetic_buffers* b, 
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     int rc = e == cudaSuccess ? MMX_OK : cuda_fail(e, "cudaStreamBeginCapture");
     if (rc == MMX_OK) {
-      rc = p->prec == MMX_C128 ? run_magnetic<double>(p, b, st, niter, cs) : run_magnetic<float>(p, b, st, niter, cs);
+      rc = run(cs);
       e = cudaStreamEndCapture(cs, &graph);
       if (rc == MMX_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
     }

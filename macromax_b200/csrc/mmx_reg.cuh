@@ -258,8 +258,12 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 }
 
 // OPS: OP_FWD (forward pass), OP_INV (inverse pass) or OP_FWD | OP_G | OP_INV (axis-0 pass with the Green multiply)
+// resident CTAs per SM the strided passes are compiled for (the register budget follows from it)
+#ifndef MMX_REG_MIN_BLOCKS
+#define MMX_REG_MIN_BLOCKS 2
+#endif
 template <int C, int OPS, int N>
-__global__ void __launch_bounds__(RegThreads<C, N>::value, 2) k_reg_pass(IterArgs<float> a) {
+__global__ void __launch_bounds__(RegThreads<C, N>::value, MMX_REG_MIN_BLOCKS) k_reg_pass(IterArgs<float> a) {
   constexpr int P = kRegP;
   constexpr int THREADS = RegThreads<C, N>::value;
   extern __shared__ __align__(16) unsigned char mmx_smem_raw[];

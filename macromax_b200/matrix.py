@@ -6,18 +6,17 @@ arguments, mode ordering, source and detection planes, vector conversions and qu
 columns are computed.  The reference solves one column at a time with a single ``Solution`` (``_matvec``,
 matrix.py:770-820; ``__array__``, matrix.py:831-844).  Here every column that is not cached is solved in one batched
 launch of the fused iteration (``BatchSolution``: all right-hand sides share the material, its preconditioner and one
-CUDA graph), in chunks that fit the device memory budget.  The mode synthesis and detection stay on the host; only
-the two source planes and the two detection planes of each column are computed, instead of whole-grid free-space
-fields.
+CUDA graph), in chunks that fit the device memory budget.  For the batched columns the mode synthesis and detection
+run on the device (transverse plane transforms by mmx_fftn, spectra scattered and gathered at the mode positions by
+mmx_mode_scatter / mmx_mode_gather); only the two source planes and the two detection planes of each column are
+computed, instead of whole-grid free-space fields.  The single-vector conversions (srcvec2freespace, ...) keep the
+host restatement.
 
 Vectors are laid out as in the reference: ``[side (front, back), mode (raster order of the propagating transverse
 k-vectors), polarisation (1 scalar, 2 vector)]``, flattened.
 
-Two differences from the reference's column loop, both only visible in ill-conditioned runs:
-- the reference re-uses one ``Solution`` whose iteration counter is never reset, so its default callback
-  (``iteration < 1e4 and residue > 1e-6``) caps the total over all columns; here each column has its own count.
-- a divergence-guard rejection raises alpha for that column only (the reference keeps the raised alpha for the
-  columns after it).
+One difference from the reference's column loop, only visible in ill-conditioned runs: a divergence-guard rejection
+raises alpha for that column only (the reference keeps the raised alpha for the columns after it).
 """
 from __future__ import annotations
 
@@ -355,7 +354,6 @@ class ScatteringMatrix:
         sol = self._solution
         sol.source_distribution = source
         sol.E = 0
-        sol.iteration = 0  # every column gets its own iteration budget (the batched columns do the same)
         sol.solve(self._callback if self._callback is not None else _default_callback)
         if out is None:
             return sol.E
@@ -436,12 +434,25 @@ class ScatteringMatrix:
 
     # -- columns: batched solves on the device ----------------------------------------------------------------------
     def _batched_outward(self, vectors: np.ndarray) -> np.ndarray:
-        """Detection vectors of the mode vectors [B, 2, P, M], all solved in batched launches.  With transverse axes
-        the mode synthesis (sources, incident fields) and the detection run on the device; ``self.timing`` keeps the
-        seconds spent in them and in the solves."""
+        """Detection vectors of the mode vectors [B, 2, P, M].  Under ``torchrun`` (a default process group of more
+        than one rank) every rank solves its ``shard_range`` slice of the columns on its own GPU and the detection
+        vectors are gathered (replicas: no collective inside the solves)."""
+        from .distributed import gather_rows, shard_range, world
+        rank, size = world()
+        if size == 1:
+            return self._outward_local(vectors)
+        a, b = shard_range(vectors.shape[0], rank, size)
+        return gather_rows(self._outward_local(vectors[a:b]), vectors.shape[0])
+
+    def _outward_local(self, vectors: np.ndarray) -> np.ndarray:
+        """Detection vectors of the mode vectors [B, 2, P, M], all solved in batched launches on this process's GPU.
+        With transverse axes the mode synthesis (sources, incident fields) and the detection run on the device;
+        ``self.timing`` keeps the seconds spent in them and in the solves."""
         nb_pol = 1 + 2 * self._vectorial
         B = vectors.shape[0]
         out = np.empty((B, self._side), dtype=self._dtype)
+        if B == 0:
+            return out
         word = np.dtype(self._dtype).itemsize
         per_rhs = 5.0 * nb_pol * self._grid.size * word  # two field buffers, work buffer, sources, staging
         chunk = int(max(1, min(self._max_batch, self._max_batch_bytes // per_rhs)))

@@ -9,9 +9,10 @@ The reference package's own ``Solution`` on the fused B200 iteration.
    device tensors, while ``ft``, ``ift``, ``norm`` and ``curl_ft`` run on this library's kernels (``mmx_fftn``,
    ``mmx_norm``, ``mmx_curl_ft``).  ``backend.load`` builds it for ``{'type': 'b200'}``.
 2. It replaces ``Solution.__iter__`` and ``Solution.solve`` (solver.py:1049-1123) with versions that, when the
-   solution's backend is that class and the medium is not magnetic, run the whole iteration body
-   (solver.py:1070-1096: chi, source, Green function, chi, norm, divergence guard, update) as the fused pass
-   kernels of ``mmx_iterate``; any other backend or a magnetic medium runs the reference's own code unchanged.
+   solution's backend is that class, run the whole iteration body (solver.py:1070-1096: chi, source, Green
+   function, chi, norm, divergence guard, update) on the device: the fused pass kernels of ``mmx_iterate``, or for
+   magnetic and bi-(an)isotropic media (chi_op of solver.py:531-552) ``mmx_magnetic_iterate``; any other backend
+   runs the reference's own code unchanged.
 
 The operator data is read from the solution's private attributes, as the reference stores them:
 ``_Solution__chiEE_base`` and ``_Solution__source_normalized`` (both at the current alpha, solver.py:474-486),
@@ -182,6 +183,19 @@ class _FusedRunner:
     def _key(t):
         return id(t), t._version, t.data_ptr()
 
+    # the runner interface shared with _MagneticRunner
+    def iterate(self, niter: int):
+        self.engine.iterate(niter)
+
+    def read_state(self) -> np.ndarray:
+        return self.engine.read_state()
+
+    def write_state(self, st: np.ndarray):
+        self.engine.write_state(st)
+
+    def run(self, rtol: float, maxiter: float) -> np.ndarray:
+        return self.engine.run(rtol, maxiter, reset_iteration=True)
+
     def sync_in(self, sol):
         """Bring the engine up to date with the solution's operators, field and update norm."""
         eng = self.engine
@@ -230,16 +244,138 @@ class _FusedRunner:
             raise ZeroDivisionError('float division by zero')
 
 
-def _runner(sol) -> _FusedRunner:
+def _blocks(t: torch.Tensor, shape) -> torch.Tensor:
+    """A 3x3 (or scalar) matrix field [r, c, *grid-broadcastable] as a new [9, N] tensor (a scalar times I)."""
+    if int(t.shape[0]) == 1 and int(t.shape[1]) == 1:
+        eye = torch.eye(3, dtype=t.dtype, device=t.device).reshape(3, 3, *([1] * len(shape)))
+        t = eye * t
+    return _matrix_rows(t, shape)
+
+
+class _MagneticRunner:
+    """The device iteration of a reference ``Solution`` for a magnetic or bi-(an)isotropic medium
+    (``mmx_magnetic_iterate``).  The reference stores its four blocks chi_EE (``_Solution__chiEE_base``), chi_EH,
+    chi_HE and chi_HH and the normalised source at the current alpha and rescales them affinely when alpha changes
+    (solver.py:514-528): the map the device iteration applies itself to blocks stored at an alpha0, so the blocks are
+    copied as they are, with alpha0 = the alpha at which they were read."""
+
+    def __init__(self, sol):
+        be = sol._Solution__BE
+        self.shape = tuple(int(s) for s in be.grid.shape)
+        self.N = int(np.prod(self.shape))
+        self.prec = nat.MMX_C64 if be.hardware_dtype == torch.complex64 else nat.MMX_C128
+        self.tdtype = be.hardware_dtype
+        self.device = be._b200_device
+        with torch.cuda.device(self.device):
+            self.plan = nat.Plan(self.shape, 1, 1, self.prec)
+            self.plan.set_kvectors([np.asarray(k, dtype=np.float64).ravel() for k in be.grid.k])
+
+            def field():
+                return torch.zeros((3, self.N), dtype=self.tdtype, device=self.device)
+
+            self.E, self.src = field(), field()
+            self.work = [field() for _ in range(7)]
+            self.blocks = [torch.zeros((9, self.N), dtype=self.tdtype, device=self.device) for _ in range(4)]
+            self.state = torch.zeros(nat.STATE_DTYPE.itemsize, dtype=torch.uint8, device=self.device)
+        self.buffers = nat.MagneticBuffers(
+            E=nat.device_ptr(self.E), src=nat.device_ptr(self.src), chi_ee=nat.device_ptr(self.blocks[0]),
+            chi_eh=nat.device_ptr(self.blocks[1]), chi_he=nat.device_ptr(self.blocks[2]),
+            chi_hh=nat.device_ptr(self.blocks[3]), work=(ctypes.c_void_p * 7)(*[t.data_ptr() for t in self.work]))
+        st = np.zeros(1, dtype=nat.STATE_DTYPE)
+        st['prev_norm'], st['rtol'], st['maxiter'], st['active'] = np.inf, -1.0, np.inf, 1
+        self.write_state(st)
+        self.material_key = None
+        self.field_key = None
+        self.prev_norm = None
+        self.iterations = 0
+
+    def read_state(self) -> np.ndarray:
+        return self.state.cpu().numpy().view(nat.STATE_DTYPE).copy()
+
+    def write_state(self, st: np.ndarray):
+        raw = np.ascontiguousarray(st, dtype=nat.STATE_DTYPE).view(np.uint8)
+        self.state.copy_(torch.from_numpy(raw.copy()).to(self.device))
+
+    @staticmethod
+    def _key(t):
+        return id(t), t._version, t.data_ptr()
+
+    def _operators(self, sol):
+        return (sol._Solution__chiEE_base, sol._Solution__chiEH, sol._Solution__chiHE, sol._Solution__chiHH,
+                sol._Solution__source_normalized)
+
+    def sync_in(self, sol):
+        ops = self._operators(sol)
+        alpha = complex(sol._Solution__alpha)
+        key = tuple(self._key(t) for t in ops) + (alpha,)
+        st = None
+        if key != self.material_key:
+            for dst, blk in zip(self.blocks, ops[:4]):
+                dst.copy_(_blocks(blk, self.shape))
+            self.src.copy_(_field_rows(ops[4], 3, self.shape))
+            st = self.read_state()
+            st['alpha_re'] = st['alpha0_re'] = alpha.real
+            st['alpha_im'] = st['alpha0_im'] = alpha.imag
+            self.material_key = key
+        E = sol._Solution__field_array
+        if self._key(E) != self.field_key:
+            self.E.copy_(_field_rows(E, 3, self.shape))
+            self.field_key = None
+        prev = float(sol._Solution__previous_update_norm)
+        if prev != self.prev_norm or st is not None:
+            st = self.read_state() if st is None else st
+            st['prev_norm'] = prev
+            self.prev_norm = prev
+        if st is not None:
+            self.write_state(st)
+
+    def iterate(self, niter: int):
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        nat.call('mmx_magnetic_iterate', self.plan.handle, ctypes.byref(self.buffers), nat.device_ptr(self.state),
+                 int(niter), 1, ctypes.c_void_p(s) if s else None)
+
+    def run(self, rtol: float, maxiter: float) -> np.ndarray:
+        st = self.read_state()
+        st['iteration'], st['rtol'], st['maxiter'], st['active'], st['status'] = 0, rtol, maxiter, 1, 0
+        self.write_state(st)
+        chunk = 8
+        while True:
+            self.iterate(chunk)
+            st = self.read_state()
+            if not st['active'][0]:
+                return st
+            chunk = min(2 * chunk, 64)
+
+    def sync_out(self, sol, st):
+        view = self.E.view(3, 1, *self.shape)
+        sol._Solution__field_array = view
+        self.field_key = self._key(view)
+        prev = float(st['prev_norm'][0])
+        sol._Solution__previous_update_norm = prev
+        self.prev_norm = prev
+        sol._Solution__relative_residue = float(st['residue'][0]) if prev > 0 else 0.0
+        alpha = complex(float(st['alpha_re'][0]), float(st['alpha_im'][0]))
+        if alpha != complex(sol._Solution__alpha):
+            sol._Solution__update_operators(alpha)
+            self.material_key = tuple(self._key(t) for t in self._operators(sol)) + (alpha,)
+        if int(st['status'][0]) == nat.MMX_STATUS_ZERODIV:
+            raise ZeroDivisionError('float division by zero')
+
+
+def _runner(sol):
     r = sol.__dict__.get('_b200_runner')
     if r is None:
-        r = _FusedRunner(sol)
+        r = _MagneticRunner(sol) if sol.magnetic else _FusedRunner(sol)
         sol.__dict__['_b200_runner'] = r
     return r
 
 
 def _fused(sol) -> bool:
-    return getattr(sol._Solution__BE, 'b200_fused', False) and not sol.magnetic
+    """Whether this solution's iteration runs on the device: a BackEndB200 (magnetic media need vector fields)."""
+    be = sol._Solution__BE
+    if not getattr(be, 'b200_fused', False):
+        return False
+    return be.vector_length == 3 if sol.magnetic else True
 
 
 def install(mm):
@@ -257,17 +393,16 @@ def install(mm):
             yield from reference_iter(self)
             return
         runner = _runner(self)
-        eng = runner.engine
         self.iteration = 0  # reset iteration counter (solver.py:1063)
-        st = eng.read_state()
+        st = runner.read_state()
         st['rtol'], st['maxiter'], st['active'], st['status'] = -1.0, np.inf, 1, 0
-        eng.write_state(st)
+        runner.write_state(st)
         while True:
             self.iteration += 1
             runner.sync_in(self)
-            eng.iterate(1)
+            runner.iterate(1)
             runner.iterations += 1
-            runner.sync_out(self, eng.read_state())
+            runner.sync_out(self, runner.read_state())
             yield self
 
     def solve(self, callback=reference_solve.__defaults__[0], rtol: float = 0, maxiter=math.inf):
@@ -284,7 +419,7 @@ def install(mm):
             rtol, maxiter = rule
         runner = _runner(self)
         runner.sync_in(self)
-        st = runner.engine.run(float(rtol), float(maxiter), reset_iteration=True)
+        st = runner.run(float(rtol), float(maxiter))
         runner.iterations += int(st['iteration'][0])
         self.iteration = int(st['iteration'][0])
         runner.sync_out(self, st)

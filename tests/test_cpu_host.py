@@ -25,6 +25,9 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, name), name
     assert set(nat.EXPORTED) <= set(names)
     assert lib.mmx_version() == 1
+    # every exported entry point has its argument types declared (64-bit counts must not pass as C ints)
+    for name in nat.EXPORTED:
+        assert getattr(lib, name).argtypes is not None, name
 
 
 def test_error_reporting_without_gpu():

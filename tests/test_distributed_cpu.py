@@ -49,3 +49,50 @@ def test_two_gloo_ranks_gather_and_max():
     for rank, full, t in results:
         assert full == [0.0, 1.0, 2.0, 3.0, 4.0, 5.0, 6.0]
         assert t == 2.0
+
+
+def _columns_worker(rank, world, port, q):
+    """Each rank of a 2-rank gloo group computes its shard of the scattering-matrix columns; the per-rank solve is
+    replaced by a host function of the mode vectors, so the partition and the gather are what is tested."""
+    import numpy as np
+    import torch.distributed as dist
+    from macromax_b200 import Grid
+    from macromax_b200.matrix import ScatteringMatrix
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        grid = Grid(shape=(32, 16), step=0.125)
+        sm = ScatteringMatrix(grid, vectorial=True, vacuum_wavelength=0.5, epsilon=1.0, dtype=np.complex128)
+        seen = []
+
+        def local(vectors):
+            seen.append(vectors.shape[0])
+            flat = vectors.reshape(vectors.shape[0], -1)
+            return (flat * (2.0 + 1.0j) + np.arange(flat.shape[1])).astype(np.complex128)
+
+        sm._outward_local = local
+        rng = np.random.default_rng(0)
+        B = 7
+        vec = rng.standard_normal((B, 2, 2, sm._modes.size)) + 1j * rng.standard_normal((B, 2, 2, sm._modes.size))
+        out = sm._batched_outward(vec)
+        q.put((rank, seen, np.allclose(out, local(vec)), out.shape))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_scattering_matrix_columns_shard_over_two_gloo_ranks():
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = 29600 + os.getpid() % 1000
+    procs = [ctx.Process(target=_columns_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    results = sorted(q.get(timeout=10) for _ in range(2))
+    # rank 0 solves columns 0..3, rank 1 columns 4..6; both end with all 7, equal to the unsharded result
+    assert [r[1][0] for r in results] == [4, 3]
+    for rank, seen, equal, shape in results:
+        assert equal and shape[0] == 7

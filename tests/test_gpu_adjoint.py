@@ -152,3 +152,28 @@ def test_adjoint_complex64_permittivity_gradient_matches_finite_differences_128(
     ga = np.array([g[idx] for idx in picks])
     err = np.linalg.norm(ga - fd) / np.linalg.norm(fd)
     assert err <= 1e-4, (err, np.max(np.abs(ga - fd) / np.abs(fd)))
+
+
+def test_mixed_precision_adjoint_matches_complex128_adjoint():
+    """precision='mixed' (complex64 inner iterations, FP64 defect correction for both solves) gives the complex128
+    adjoint gradient of the same problem within 1e-7 relative, for the permittivity and the sources, in a batch."""
+    import torch
+    from macromax_b200 import adjoint
+    wl, grid, bound = _problem()
+    k0 = 2 * np.pi / wl['wavelength']
+    grads = {}
+    # the same complex128 inputs for both (the mixed solve's own arithmetic is complex64 inside, FP64 outside)
+    for name, dt, tdt, kw in (('c128', np.complex128, torch.complex128, dict(rtol=1e-12)),
+                              ('mixed', np.complex128, torch.complex128, dict(rtol=1e-12, precision='mixed'))):
+        eps = torch.tensor(wl['epsilon'], dtype=tdt, device='cuda', requires_grad=True)
+        base = torch.tensor(wl['source'], dtype=tdt, device='cuda')
+        src = torch.stack([base, 0.5 * torch.roll(base, 3, dims=2)]).requires_grad_(True)
+        E = adjoint.solve(eps, src, grid, k0, bound=bound, dtype=dt, maxiter=20000, **kw)
+        L = sum(_loss(E[b:b + 1], wl['patch']) for b in range(2))
+        L.backward()
+        assert eps.grad.dtype == tdt and src.grad.dtype == tdt
+        grads[name] = (eps.grad.detach().cpu().numpy().astype(np.complex128),
+                       src.grad.detach().cpu().numpy().astype(np.complex128))
+    for k in range(2):
+        a, b = grads['mixed'][k], grads['c128'][k]
+        assert np.linalg.norm(a - b) <= 1e-7 * np.linalg.norm(b)

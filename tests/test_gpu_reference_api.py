@@ -142,3 +142,26 @@ def test_reference_backend_conformance_suite(method):
     TestBackEndB200(method).run(result)
     problems = result.failures + result.errors
     assert not problems, problems[0][1]
+
+
+@pytest.mark.parametrize('name', ['magnetic2d_48_c128', 'chiral3d_16_c128'])
+def test_reference_magnetic_solution_iterates_on_b200(name):
+    """Magnetic and bi-(an)isotropic media through the reference's own Solution on 'b200': the iteration runs on
+    mmx_magnetic_iterate with the reference's stored blocks; iterates within 1e-10 of the reference NumPy backend's
+    fixtures, and the final alpha."""
+    mm = _mm()
+    z = load_golden(name)
+    grid = mm.Grid(shape=tuple(int(s) for s in z['shape']), step=float(z['step']))
+    sol = mm.Solution(grid, vacuum_wavelength=float(z['wavelength']), epsilon=z['epsilon'], xi=z['xi'],
+                      zeta=z['zeta'], mu=z['mu'], source_distribution=z['source'],
+                      bound=mm.bound.Bound(grid, thickness=float(z['bound_thickness'])), dtype=np.complex128)
+    assert sol.magnetic
+    assert abs(complex(sol._Solution__alpha) - complex(z['alpha0'])) <= 1e-12 * abs(complex(z['alpha0']))
+    record = set(int(r) for r in z['record'])
+    for s in sol:
+        if s.iteration in record:
+            assert rel(s.E, z[f'E{s.iteration}']) < 1e-10, s.iteration
+        if s.iteration >= max(record):
+            break
+    assert complex(sol._Solution__alpha) == pytest.approx(complex(z['alpha_final']), rel=1e-12)
+    assert sol.__dict__['_b200_runner'].iterations == sol.iteration
