@@ -153,6 +153,41 @@ def cpu_torch_rate(wl, dtype, iters: int):
     return int(np.prod(wl['shape'])) * iters / dt, dt, torch.get_num_threads()
 
 
+def reference_package_rates(wl, iters: int):
+    """The reference package's own Solution (python/macromax/solver.py) on its NumPy and torch-CPU backends, on the
+    same workload and host cores: voxel-iterations/s over ``iters`` iterations after one warm-up iteration, and the
+    set-up time.  None where the package is not present (it is read from baseline/_ref)."""
+    import torch
+    from oracle.refimport import import_reference, reference_available
+    if not reference_available():
+        return None
+    mm = import_reference()
+    out = {}
+    nvox = int(np.prod(wl['shape']))
+    for name, cfg in (('numpy', {'type': 'numpy'}), ('torch_cpu', {'type': 'torch', 'device': 'cpu'})):
+        mm.backend.config(cfg)
+        grid = mm.Grid(shape=wl['shape'], step=wl['step'])
+        t0 = time.perf_counter()
+        sol = mm.Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
+                          source_distribution=wl['source'], bound=mm.bound.Bound(grid, thickness=wl['bound_thickness']),
+                          dtype=np.complex64)
+        t1 = time.perf_counter()
+        it = iter(sol)
+        next(it)  # warm-up iteration
+        t2 = time.perf_counter()
+        for _ in range(iters):
+            next(it)
+        dt = time.perf_counter() - t2
+        # numpy.fft runs on one thread; torch uses its intra-op thread pool
+        out[name] = {'value': nvox * iters / dt, 'unit': UNIT, 'setup_s': t1 - t0, 'kind': 'reference',
+                     'cores': 1 if name == 'numpy' else torch.get_num_threads(),
+                     'sample': f'{iters} iterations of the reference package\'s Solution on its {name} backend '
+                               f'after one warm-up iteration ({dt:.1f} s)'}
+        del sol, it
+    mm.backend.config({'type': 'numpy'})
+    return out
+
+
 def bench_reference(args, wl, rank, world, pg):
     """--impl reference: the oracle's iteration on the host cores, one iteration per step."""
     dtype = np.complex64
@@ -273,6 +308,12 @@ def bench_ours(args, wl, rank, world, local, pg):
             cpu['torch_cpu'] = {'value': trate, 'unit': UNIT, 'cores': threads, 'kind': 'port',
                                 'sample': f'{args.cpu_iters} iterations with torch CPU tensors on the full workload '
                                           f'({tdt:.1f} s), {threads} threads'}
+        try:
+            ref_pkg = reference_package_rates(wl, 3)
+        except Exception as e:  # the reference package is optional here; its absence or failure is reported
+            ref_pkg = {'unavailable': f'{type(e).__name__}: {e}'[:200]}
+        if ref_pkg is not None:
+            cpu['reference_package'] = ref_pkg
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,

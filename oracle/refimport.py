@@ -1,5 +1,6 @@
 """
-Import the reference ``macromax`` package for fixture generation (and for the optional CPU-side integration test).
+Import the reference ``macromax`` package: for fixture generation (tests/golden/make_golden.py), the tests that run
+the reference's own API and test suite on this library, and the CPU baseline of bench.py.  Test infrastructure.
 
 The reference package writes a log file next to itself on import (``macromax/__init__.py:61-67``) and needs
 ``coloredlogs`` and installed package metadata, neither of which exists here.  So this helper copies the package to
@@ -17,7 +18,7 @@ import shutil
 import sys
 import tempfile
 
-_REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+_REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REFERENCE_PYTHON = os.environ.get('MACROMAX_REFERENCE', os.path.join(_REPO, 'baseline', '_ref'))
 
 _STUB = '''

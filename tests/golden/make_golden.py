@@ -26,7 +26,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from refimport import import_reference  # noqa: E402
+from oracle.refimport import import_reference  # noqa: E402
 from macromax_b200 import workloads  # noqa: E402
 
 RECORD = (1, 2, 3, 5, 10, 20)

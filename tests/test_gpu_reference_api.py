@@ -13,8 +13,6 @@ by ``macromax_b200.backend.register`` (``refhook``).
 
 The reference package is read from ``baseline/_ref`` (or ``$MACROMAX_REFERENCE``); without it these tests skip.
 """
-import os
-import sys
 import unittest
 
 import numpy as np
@@ -24,8 +22,8 @@ from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
-from refimport import import_reference, load_reference_test_module, reference_available, reference_tests_dir  # noqa
+from oracle.refimport import (import_reference, load_reference_test_module, reference_available,  # noqa: E402
+                              reference_tests_dir)
 
 
 def _mm():

@@ -9,10 +9,7 @@ import pytest
 
 
 def _reference():
-    import os
-    import sys
-    sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
-    from refimport import import_reference, reference_available
+    from oracle.refimport import import_reference, reference_available
     if not reference_available():
         pytest.skip('reference package not present on this machine')
     return import_reference()
