@@ -174,7 +174,7 @@ int mmx_pointwise_mul(const void* A, int ra, int ca, const void* B, int cb, int 
 #define MMX_VARIANT_SHARED_STAGED 2u  /* compile-time kernels without the register-staged passes */
 #define MMX_VARIANT_PERSISTENT 4u     /* persistent double-buffered prologue/epilogue passes */
 #define MMX_VARIANT_PLANE 8u          /* 3D, 128 x 128 planes, isotropic chi: the two inner axes in one pass */
-#define MMX_VARIANT_FUSED_EPILOGUE 16u /* isotropic chi: epilogue fused with the next prologue (speculative) */
+#define MMX_VARIANT_FUSED_EPILOGUE 16u /* epilogue fused with the next prologue (speculative); isotropic chi, and a 3x3 chi on 192-sample rows */
 #define MMX_VARIANT_TMA 32u            /* strided 128-sample passes staged by bulk tensor (TMA) copies */
 
 /* Select the kernel variant of a plan (rebuilds its pass list, drops its captured graphs).  No reference

@@ -101,7 +101,7 @@ struct PassCfg {
   int regc = 0;  // 1: register-staged contiguous prologue/epilogue pass (k_regc_pass) for an isotropic chi
   int pipe = 0;  // 1: persistent double-buffered variant of the same pass (k_pipe_pass)
   int plane = 0; // 1: plane pass over the two inner axes of a 3D grid (k_plane_pass), 2-CTA clusters
-  int epro = 0;  // 1: epilogue fused with the next iteration's speculative prologue (k_regc_epro)
+  int epro = 0;  // 1: epilogue fused with the next iteration's speculative prologue (k_regc_epro, k_regc_aniso_epro)
   int repair = 0;  // 1: prologue again for rejected right-hand sides (k_regc_repair)
   int regc_aniso = 0;  // 1: register-staged contiguous pass for a 3x3 chi (k_regc_aniso_pass), rc_tiles / rc_smem
   int64_t rc_tiles = 0;
@@ -146,7 +146,7 @@ struct mmx_plan {
   int poll_limit = 1 << 20;
   bool plane = false;          // plane passes over the two inner axes (3D, 128 x 128 planes, isotropic chi)
   std::vector<PassCfg> plane_passes;  // the 3-pass schedule used when `plane` is set and chi is isotropic
-  bool epro = false;           // fuse each epilogue with the next iteration's prologue (isotropic chi)
+  bool epro = false;           // fuse each epilogue with the next iteration's prologue
   bool tma = false;            // strided 128-sample passes staged by bulk tensor copies (k_tma_pass)
   std::vector<PassCfg> epro_passes;   // [middle passes..., EPI+PRO, repair]; the first PRO runs once per call
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
@@ -516,13 +516,53 @@ int launch_repair(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t 
   }
 }
 
+// the fused epilogue / prologue and the repair pass for a 3x3 chi (k_regc_aniso_epro, k_regc_aniso_repair)
+template <int N, int CHI>
+int launch_aniso_epro(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  constexpr int PCK = RegCDefault<3, N>::PC;
+  auto kern = k_regc_aniso_epro<N, PCK, CHI>;
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  a.nrhs = batch;
+  dim3 grid((unsigned)pc.rc_tiles, (unsigned)batch);
+  MMX_CUDA(launch_pass(kern, grid, dim3(RegC<3, N, PCK>::THREADS), pc.rc_smem, s, a));
+  return MMX_OK;
+}
+
+template <int N, int CHI>
+int launch_aniso_repair(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  constexpr int PCK = RegCDefault<3, N>::PC;
+  auto kern = k_regc_aniso_repair<N, PCK, CHI>;
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  a.nrhs = batch;
+  const int64_t grid = std::min<int64_t>(pc.rc_tiles, (int64_t)sm_count());
+  MMX_CUDA(launch_pass(kern, dim3((unsigned)grid), dim3(RegC<3, N, PCK>::THREADS), pc.rc_smem, s, a,
+                       (int)pc.rc_tiles));
+  return MMX_OK;
+}
+
 template <int C, int CHI, int N>
 int fast_ops(const PassCfg& pc, const IterArgs<float>& a, int batch, cudaStream_t s) {
   if (pc.epro || pc.repair) {
     if constexpr (CHI == MMX_CHI_SCALAR) {
-      return pc.epro ? launch_epro<C, N>(pc, a, batch, s) : launch_repair<C, N>(pc, a, batch, s);
+      if (!pc.regc_aniso)
+        return pc.epro ? launch_epro<C, N>(pc, a, batch, s) : launch_repair<C, N>(pc, a, batch, s);
+    } else if constexpr (C == 3 && N == 192) {
+      if (pc.regc_aniso)
+        return pc.epro ? launch_aniso_epro<N, CHI>(pc, a, batch, s) : launch_aniso_repair<N, CHI>(pc, a, batch, s);
     }
-    return fail(MMX_ERR_ARG, "internal: fused epilogue pass with an anisotropic chi");
+    return fail(MMX_ERR_ARG, "internal: fused epilogue pass for another kind of chi");
   }
   if (pc.plane) {
     if constexpr (CHI == MMX_CHI_SCALAR && N == mmx_plane::N) {
@@ -744,12 +784,16 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
 // The per-iteration passes with the epilogue fused to the next iteration's speculative prologue: the middle
 // passes of the plain schedule, then [INV EPI + PRO FWD] and the repair pass (empty when the contiguous axis has no
 // register-staged kernel).  The plain schedule's first pass runs once at the start of every chunk of iterations.
+// The list serves an isotropic chi, or a 3x3 chi when its passes carry regc_aniso (epro_serves below).
 std::vector<PassCfg> build_epro_passes(const mmx_plan* p) {
   std::vector<PassCfg> v;
   if (p->ndim < 2 || p->prec != MMX_C64 || p->force_generic) return v;
   const std::vector<PassCfg> plain = build_passes(p, false);
-  if (plain.size() < 3 || !plain.front().regc || !plain.back().regc || plain.front().pipe || plain.back().pipe)
-    return v;
+  if (plain.size() < 3) return v;
+  // isotropic chi (k_regc_epro) or a 3x3 chi (k_regc_aniso_epro; the passes keep their regc_aniso flag)
+  const bool iso = plain.front().regc && plain.back().regc && !plain.front().pipe && !plain.back().pipe;
+  const bool aniso = plain.front().regc_aniso && plain.back().regc_aniso;
+  if (!iso && !aniso) return v;
   for (size_t k = 1; k + 1 < plain.size(); ++k) v.push_back(plain[k]);
   PassCfg epi = plain.back();
   epi.regc = 0;
@@ -787,6 +831,12 @@ std::vector<PassCfg> build_plane_passes(const mmx_plan* p) {
   return v;
 }
 
+// whether the plan's fused-epilogue passes apply to this kind of chi
+bool epro_serves(const mmx_plan* p, int chi_kind) {
+  if (p->epro_passes.empty()) return false;
+  return p->epro_passes.back().regc_aniso ? chi_kind != MMX_CHI_SCALAR : chi_kind == MMX_CHI_SCALAR;
+}
+
 template <class R> IterArgs<R> base_args(mmx_plan* p) {
   IterArgs<R> a;
   memset(&a, 0, sizeof(a));
@@ -817,8 +867,7 @@ int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kin
   // the accept/reject decision is taken by the last tile of the epilogue pass (no separate launch)
   const bool plane = std::is_same<R, float>::value && p->plane && chi_kind == MMX_CHI_SCALAR &&
                      !p->plane_passes.empty();
-  const bool epro = std::is_same<R, float>::value && !plane && p->epro && chi_kind == MMX_CHI_SCALAR &&
-                    !p->epro_passes.empty();
+  const bool epro = std::is_same<R, float>::value && !plane && p->epro && epro_serves(p, chi_kind);
   if (epro) {
     // first prologue of the chunk, then per iteration the middle passes, the fused epilogue + next prologue and
     // the repair pass

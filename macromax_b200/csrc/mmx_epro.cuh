@@ -264,3 +264,157 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (RegCMinBlocks<C, OP_
     }
   }
 }
+
+// ---------------------------------------------------------------------------------------------------------------
+// The same fusion for a 3x3 chi (MMX_CHI_SYM6 / MMX_CHI_MAT3) on rows of k_regc_aniso_pass's lengths (192).
+//
+// The epilogue stage of k_regc_aniso_pass already gives one thread all three components of a voxel and the voxel's
+// chi entries, so after E' = E + chi (T - E) the thread forms the next iteration's input x = chi(alpha) E' + s'
+// from the same chi words (the operations in the order of the prologue's) and writes it over the inverse
+// transform's output, at the positions it has just read.  The forward transform then runs from shared memory in
+// the per-component layout and its last stage writes T.  Per voxel and iteration the six (or nine) chi words and E'
+// are read once instead of twice, and one pass over the grid is saved.  The prologue is speculative as above;
+// k_regc_aniso_repair redoes it for a right-hand side whose update was rejected.
+// ---------------------------------------------------------------------------------------------------------------
+// Measured on the 192^3 anisotropic iteration (582.8 us against 617.8 us for the plain passes): four 192-thread CTAs
+// per SM at 80 registers.  Five CTAs (64 registers: spills) took 664-700 us; three CTAs with the chi stage unrolled
+// four times 613 us; the first inverse stage's loads all issued at once 592 us; L2 bulk prefetches of the tile's chi,
+// s' and E rows 587-590 us.
+template <int N, int PC_, int CHI>
+__global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_epro(IterArgs<float> a) {
+  constexpr int C = 3;
+  using G = RegC<C, N, PC_>;
+  using Plan = typename RegPlan<N>::type;
+  using PA = RegPlanArgs<Plan>;
+  constexpr int TPP = G::TPP, PC = G::PC, THREADS = G::THREADS;
+  constexpr int M = CHI == MMX_CHI_SYM6 ? 6 : 9;
+  constexpr int RAD = PA::R_first;
+  constexpr int T1 = N / RAD;  // first-stage butterflies per row
+  static_assert(T1 == C * TPP, "one (row, butterfly slot) item per thread");
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + C * PC * G::PITCH;
+  const int b = blockIdx.y;
+  const mmx_rhs_state* st = a.st + b;
+  const int64_t N3 = a.N;
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
+  const ChiCoef<float> cc = chi_coef<float>(st);
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;          // per-component layout (FFT stages)
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int irow = tid / T1;         // all-component layout (chi stage): row and butterfly slot
+  const int islot = tid % T1;
+  const int64_t fbase = (int64_t)b * C * N3;
+  const int cur = st->cur;
+  const float2* __restrict__ Ecur = cur ? a.E1 : a.E0;
+  float2* __restrict__ Eoth = cur ? a.E0 : a.E1;
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
+  __syncthreads();
+  const int64_t ibase = ((int64_t)blockIdx.x * PC + irow) * N;  // voxel of sample 0 of the item's row
+  const float2* __restrict__ eI = Ecur + fbase + ibase;          // component r at eI[r N3 + sample]
+  const float2* __restrict__ xI = a.chi + ibase;                 // entry k at xI[k N3 + sample]
+  const float2* __restrict__ sI = a.src + fbase + ibase;
+  float2* __restrict__ eO = Eoth + fbase + ibase;
+  float2* __restrict__ trow = a.T + fbase + c * N3 + ((int64_t)blockIdx.x * PC + row) * N;
+  constexpr int RL = PA::R_last;
+  constexpr int TL = N / RL;
+  constexpr int NBL = TL / TPP;
+  // inverse transform of T: first stage from global memory, middle stages, last stage back to the positions it read
+  {
+    constexpr int NBT = T1 / TPP;
+#pragma unroll 1
+    for (int mm = 0; mm < NBT; ++mm) {
+      const int i = ii + mm * TPP;
+      float2 v[RAD];
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) v[q] = trow[i + q * T1];
+      bfly<float, RAD, +1>(v, smtw, N);
+#pragma unroll
+      for (int q = 0; q < RAD; ++q) sm[G::idx(c, row, i * RAD + q)] = v[q];
+    }
+  }
+  __syncthreads();
+  PA::template mid<+1, N, C, PC>(sm, smtw);
+#pragma unroll 1
+  for (int mm = 0; mm < NBL; ++mm) {
+    const int i = ii + mm * TPP;
+    float2 v[RL];
+#pragma unroll
+    for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+    for (int q = 1; q < RL; ++q) v[q] = v[q] * conjc(smtw[q * i]);
+    bfly<float, RL, +1>(v, smtw, N);
+#pragma unroll
+    for (int q = 0; q < RL; ++q) sm[G::idx(c, row, i + q * TL)] = v[q];
+  }
+  __syncthreads();
+  // epilogue and speculative prologue, all three components of a voxel per thread
+  bool with_src[C];
+#pragma unroll
+  for (int r = 0; r < C; ++r) with_src[r] = !source_is_zero(st, r);
+  double dd2 = 0.0, en2 = 0.0;
+#pragma unroll 2
+  for (int q = 0; q < N / T1; ++q) {
+    const int s_ = islot + q * T1;
+    float2 e[C], diff[C], en[C], m[M];
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      e[r] = eI[r * N3 + s_];
+      diff[r] = sm[G::idx(r, irow, s_)] - e[r];
+    }
+#pragma unroll
+    for (int k = 0; k < M; ++k) m[k] = cc.a * xI[k * N3 + s_];
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      float2 d = cc.b * diff[r];
+#pragma unroll
+      for (int s2 = 0; s2 < C; ++s2) d += m[chi_entry<CHI>(r, s2)] * diff[s2];
+      en[r] = e[r] + d;
+      eO[r * N3 + s_] = en[r];
+      dd2 += norm2d(d);
+      en2 += norm2d(en[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      float2 acc = cc.b * en[r];
+      if (with_src[r]) acc += cc.s * sI[r * N3 + s_];
+#pragma unroll
+      for (int s2 = 0; s2 < C; ++s2) acc += m[chi_entry<CHI>(r, s2)] * en[s2];
+      sm[G::idx(r, irow, s_)] = acc;  // a position this thread has read above
+    }
+  }
+  __syncthreads();
+  CChainToGlobal<-1, N, C, PC, 1, Plan>::run(sm, smtw, trow);
+  finish_pass_norms(a, b, dd2, en2);
+}
+
+// Prologue pass again, for a 3x3 chi, for every right-hand side whose last update was rejected (grid-stride over
+// its tiles; the CTAs leave at once when every update was accepted).
+template <int N, int PC_, int CHI>
+__global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_repair(IterArgs<float> a,
+                                                                                   int tiles_per_rhs) {
+  using G = RegC<3, N, PC_>;
+  constexpr int THREADS = G::THREADS;
+  extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
+  float2* smtw = sm + 3 * G::PC * G::PITCH;
+  const float2* twg = (const float2*)a.ax.tw;
+  for (int t = threadIdx.x; t < N; t += THREADS) smtw[t] = twg[t];
+  pdl_wait();
+  pdl_trigger();
+  __syncthreads();
+  for (int b = 0; b < a.nrhs; ++b) {
+    const mmx_rhs_state* st = a.st + b;
+    if (!st->active || st->accepted) continue;  // uniform over the CTA
+    const ChiCoef<float> cc = chi_coef<float>(st);
+    const float2* Ecur = st->cur ? a.E1 : a.E0;
+    for (int64_t t = blockIdx.x; t < tiles_per_rhs; t += gridDim.x) {
+      aniso_pro_tile<N, PC_, CHI>(a, b, t, sm, smtw, cc, Ecur);
+      __syncthreads();  // the tile's shared memory is free again
+    }
+  }
+}

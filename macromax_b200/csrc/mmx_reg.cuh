@@ -737,6 +737,77 @@ template <int CHI> __device__ __forceinline__ int chi_entry(int r, int s) {
   }
 }
 
+// The prologue of one tile (PC rows) of right-hand side b for a 3x3 chi: x = chi(alpha) E + s'(alpha) formed as the
+// first radix stage loads it (one thread per (row, butterfly slot), all three components), the forward FFT along
+// the contiguous axis, written to T.  Expects the twiddles in smtw and the tile's shared memory free.
+template <int N, int PC_, int CHI>
+__device__ __forceinline__ void aniso_pro_tile(const IterArgs<float>& a, int b, int64_t tile, float2* sm,
+                                               const float2* smtw, const ChiCoef<float>& cc, const float2* Ecur) {
+  constexpr int C = 3;
+  using G = RegC<C, N, PC_>;
+  using PA = RegPlanArgs<typename RegPlan<N>::type>;
+  constexpr int TPP = G::TPP, PC = G::PC;
+  constexpr int M = CHI == MMX_CHI_SYM6 ? 6 : 9;
+  constexpr int RAD = PA::R_first;
+  constexpr int T1 = N / RAD;
+  static_assert(T1 == C * TPP, "one (row, butterfly slot) item per thread");
+  constexpr int RL = PA::R_last;
+  constexpr int TL = N / RL;
+  constexpr int NBL = TL / TPP;
+  const mmx_rhs_state* st = a.st + b;
+  const int tid = threadIdx.x;
+  const int ii = tid % TPP;
+  const int row = (tid / TPP) % PC;
+  const int c = tid / (TPP * PC);
+  const int irow = tid / T1;
+  const int islot = tid % T1;
+  const int64_t N3 = a.N;
+  const int64_t fbase = (int64_t)b * C * N3;
+  const int64_t ibase = (tile * PC + irow) * N;
+  const float2* __restrict__ eI = Ecur + fbase + ibase;
+  const float2* __restrict__ xI = a.chi + ibase;
+  const float2* __restrict__ sI = a.src + fbase + ibase;
+  float2 u[C][RAD];
+#pragma unroll
+  for (int q = 0; q < RAD; ++q) {
+    const int s_ = islot + q * T1;
+    float2 e[C], m[M];
+#pragma unroll
+    for (int r = 0; r < C; ++r) e[r] = eI[r * N3 + s_];
+#pragma unroll
+    for (int k = 0; k < M; ++k) m[k] = cc.a * xI[k * N3 + s_];
+#pragma unroll
+    for (int r = 0; r < C; ++r) {
+      float2 acc = cc.b * e[r];
+      if (!source_is_zero(st, r)) acc += cc.s * sI[r * N3 + s_];
+#pragma unroll
+      for (int s2 = 0; s2 < C; ++s2) acc += m[chi_entry<CHI>(r, s2)] * e[s2];
+      u[r][q] = acc;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < C; ++r) {
+    bfly<float, RAD, -1>(u[r], smtw, N);
+#pragma unroll
+    for (int q = 0; q < RAD; ++q) sm[G::idx(r, irow, islot * RAD + q)] = u[r][q];
+  }
+  __syncthreads();
+  PA::template mid<-1, N, C, PC>(sm, smtw);
+  float2* __restrict__ tO = a.T + fbase + c * N3 + (tile * PC + row) * N;
+#pragma unroll 1
+  for (int mm = 0; mm < NBL; ++mm) {
+    const int i = ii + mm * TPP;
+    float2 v[RL];
+#pragma unroll
+    for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
+#pragma unroll
+    for (int q = 1; q < RL; ++q) v[q] = v[q] * smtw[q * i];
+    bfly<float, RL, -1>(v, smtw, N);
+#pragma unroll
+    for (int q = 0; q < RL; ++q) tO[i + q * TL] = v[q];
+  }
+}
+
 template <int OPS, int N, int PC_, int CHI>
 __global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_pass(IterArgs<float> a) {
   constexpr int C = 3;
@@ -780,46 +851,7 @@ __global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_pass
   constexpr int NBL = TL / TPP;
 
   if constexpr (OPS == (OP_PRO | OP_FWD)) {
-    const float2* __restrict__ sI = a.src + fbase + ibase;
-    float2 u[C][RAD];
-#pragma unroll
-    for (int q = 0; q < RAD; ++q) {
-      const int s_ = islot + q * T1;
-      float2 e[C], m[M];
-#pragma unroll
-      for (int r = 0; r < C; ++r) e[r] = eI[r * N3 + s_];
-#pragma unroll
-      for (int k = 0; k < M; ++k) m[k] = cc.a * xI[k * N3 + s_];
-#pragma unroll
-      for (int r = 0; r < C; ++r) {
-        float2 acc = cc.b * e[r];
-        if (!source_is_zero(st, r)) acc += cc.s * sI[r * N3 + s_];
-#pragma unroll
-        for (int s2 = 0; s2 < C; ++s2) acc += m[chi_entry<CHI>(r, s2)] * e[s2];
-        u[r][q] = acc;
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < C; ++r) {
-      bfly<float, RAD, -1>(u[r], smtw, N);
-#pragma unroll
-      for (int q = 0; q < RAD; ++q) sm[G::idx(r, irow, islot * RAD + q)] = u[r][q];
-    }
-    __syncthreads();
-    PA::template mid<-1, N, C, PC>(sm, smtw);
-    float2* __restrict__ tO = a.T + fbase + c * N3 + ((int64_t)blockIdx.x * PC + row) * N;
-#pragma unroll 1
-    for (int mm = 0; mm < NBL; ++mm) {
-      const int i = ii + mm * TPP;
-      float2 v[RL];
-#pragma unroll
-      for (int q = 0; q < RL; ++q) v[q] = sm[G::idx(c, row, i + q * TL)];
-#pragma unroll
-      for (int q = 1; q < RL; ++q) v[q] = v[q] * smtw[q * i];
-      bfly<float, RL, -1>(v, smtw, N);
-#pragma unroll
-      for (int q = 0; q < RL; ++q) tO[i + q * TL] = v[q];
-    }
+    aniso_pro_tile<N, PC_, CHI>(a, b, blockIdx.x, sm, smtw, cc, Ecur);
   } else {
     // INV | EPI: the inverse transform in the per-component layout, its outputs back in shared memory at their
     // natural positions, then the epilogue in the all-component layout

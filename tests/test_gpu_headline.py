@@ -186,3 +186,45 @@ def test_zero_source_components_are_skipped_without_changing_the_iterates(sphere
         fields.append(sol.E)
         eng.close()
     assert np.array_equal(fields[0], fields[1])
+
+
+def test_anisotropic_192_fused_epilogue_matches_oracle_and_plain_schedule():
+    """The 3x3-chi epilogue fused with the next prologue on 192-sample rows (variant 16: k_regc_aniso_epro, with
+    k_regc_aniso_repair after a rejection) against the oracle's iterates at 1, 5 and 20 iterations, and against the
+    plain schedule (k_regc_aniso_pass) of the same plan."""
+    wl = _stacked_voronoi(2)
+    alpha_ref, ref = _oracle_fields(wl)
+    alpha, fields = _device_fields(wl, 16)
+    _, plain = _device_fields(wl, 0)
+    assert abs(alpha - alpha_ref) <= 1e-9 * abs(alpha_ref)
+    for it in RECORD:
+        assert rel(fields[it], ref[it]) < 1e-5, (it, rel(fields[it], ref[it]))
+        assert rel(fields[it], plain[it]) < 2e-6, (it, rel(fields[it], plain[it]))
+
+
+def _anisotropic_gain():
+    """The stacked Voronoi medium (192 samples on the contiguous axis) with a gain block (-0.5i on the diagonal of
+    chi): the oracle rejects 10 of the first 40 updates and raises alpha."""
+    wl = _stacked_voronoi(2)
+    eps = wl['epsilon'].copy()
+    for c in range(3):
+        eps[c, c, 24:40, 24:40, 88:104] -= 0.5j
+    return {**wl, 'epsilon': eps}
+
+
+def test_anisotropic_192_fused_epilogue_with_rejections():
+    """Rejected updates on the 3x3-chi path: the repair pass recomputes the prologue from the kept field at the
+    raised alpha.  Same rejections and alpha as the oracle and the plain schedule, and no further from the complex128
+    oracle than the plain schedule (the gain amplifies the rounding of either complex64 schedule)."""
+    from oracle import mmoracle as mo
+    wl = _anisotropic_gain()
+    mo.set_fft_workers(os.cpu_count() or 1)
+    ref = mo.from_workload(wl, np.complex128)
+    rec = ref.solve(rtol=0, maxiter=40, record=(40,))
+    a, st_a = _solve_variant(wl, 16, 40)
+    b, st_b = _solve_variant(wl, 0, 40)
+    assert int(st_a['status'][0]) == 0 and int(st_a['iteration'][0]) == 40
+    assert int(st_a['rejections'][0]) == int(st_b['rejections'][0]) == ref.rejections > 0
+    assert abs(st_a['alpha_im'][0] - ref.alpha.imag) <= 1e-9 * abs(ref.alpha.imag)
+    ea, eb = rel(a, rec[40]), rel(b, rec[40])
+    assert ea <= 2.0 * eb + 1e-6, (ea, eb)
