@@ -458,10 +458,9 @@ def run_secondary(args):
                        vacuum_wavelength=wl['wavelength'])
     torch.cuda.synchronize()
     b = time.perf_counter()
-    # the inner iteration's kernel variant: the plain 3x3-chi passes or the fused epilogue (timed trials, restored)
-    from macromax_b200 import autotune
-    tuned3 = autotune.tune(ms.inner.engine, iters=10, use_cache=False,
-                           candidates=(0, nat.MMX_VARIANT_FUSED_EPILOGUE))
+    # the inner iteration's kernel variant: the plain 3x3-chi passes or the fused epilogue (timed trials on the
+    # problem's own sources, then restored)
+    tuned3 = ms.tune(iters=10, candidates=(0, nat.MMX_VARIANT_FUSED_EPILOGUE))
     torch.cuda.synchronize()
     b = time.perf_counter()
     ms.solve(rtol=1e-8)

@@ -67,7 +67,11 @@ def get_variant(engine) -> int:
 
 
 def tune(engine, iters: int = 20, use_cache: bool = True, candidates=CANDIDATES) -> dict:
-    """Pick and apply the fastest variant for ``engine``; returns {'variant', 'us_per_iteration', 'trials'}."""
+    """Pick and apply the fastest variant for ``engine``; returns {'variant', 'us_per_iteration', 'trials'}.
+
+    The trials run the engine's own right-hand sides.  A trial counts only if every right-hand side took all its
+    timed iterations: an engine whose sources and fields are zero (0 / 0 residue) stops at once and would time empty
+    launches, so it raises ``RuntimeError`` instead (set its sources first)."""
     key = problem_key(engine)
     cache = _load() if use_cache else {}
     if use_cache and key in cache:
@@ -89,13 +93,22 @@ def tune(engine, iters: int = 20, use_cache: bool = True, candidates=CANDIDATES)
             engine.prepare_graph(iters)
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            before = engine.read_state()['iteration'].copy()
             a.record(stream)
             engine.iterate(iters)
             b.record(stream)
             torch.cuda.synchronize()
+            after = engine.read_state()
+            if not np.all(after['iteration'] - before == iters):
+                continue  # some right-hand side stopped: the time is not that of full iterations
             trials[str(flags)] = a.elapsed_time(b) * 1e3 / iters
         except nat.NativeError:
             continue
+    if not trials:
+        engine.fields.copy_(fields)
+        engine.state.copy_(state)
+        raise RuntimeError('autotune: no variant ran its iterations on every right-hand side '
+                           '(zero sources, or a diverging state?)')
     best = min(trials, key=trials.get)
     engine.fields.copy_(fields)
     engine.state.copy_(state)

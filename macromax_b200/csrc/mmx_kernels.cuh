@@ -46,6 +46,8 @@ template <class R> struct IterArgs {
   size_t l2_window;      // bytes of T kept L2-resident (0: off); host-side launch attribute only
   int nrhs;              // number of right-hand sides (persistent passes)
   int poll_limit;        // polls of a staged-input wait before the pass falls back to global loads (k_pipe_pass)
+  int csplit;            // > 1: a one-component strided pass over the csplit components of each RHS, which
+                         //      blockIdx.y enumerates (RHS-major); 0 or 1: blockIdx.y is the RHS
 };
 
 // Programmatic dependent launch.  The pass kernels are launched so that the next pass's CTAs may become resident

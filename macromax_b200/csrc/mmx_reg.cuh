@@ -269,7 +269,10 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, MMX_REG_MIN_BLOCKS) k
   extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
   float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
   float2* smtw = sm + C * N * P;
-  const int b = blockIdx.y;
+  // component split (one-component kernel on a vector field): blockIdx.y = RHS * csplit + component
+  const bool split = C == 1 && a.csplit > 1;
+  const int b = split ? (int)blockIdx.y / a.csplit : (int)blockIdx.y;
+  const int64_t field0 = split ? (int64_t)blockIdx.y : (int64_t)b * C;  // first component plane of the tile
   const mmx_rhs_state* st = a.st + b;
   pdl_wait();
   pdl_trigger();
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, MMX_REG_MIN_BLOCKS) k
   const int64_t p0 = (int64_t)blockIdx.x * P;
   const int64_t o = p0 / inner;
   const int64_t in0 = p0 - o * inner;
-  float2* tile = a.T + (int64_t)b * C * a.N + o * (int64_t)N * inner + in0;
+  float2* tile = a.T + field0 * a.N + o * (int64_t)N * inner + in0;
   const float2* twg = (const float2*)a.ax.tw;
   for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
   __syncthreads();
@@ -419,7 +422,7 @@ template <int C, int N> struct RegCDefault {
   // prologue and epilogue tiles: at most 256 threads per CTA, several CTAs per SM
   static constexpr int P0 = 256 / (C * TPP);
   static constexpr int PC = P0 >= 32 ? 32 : P0 >= 16 ? 16 : P0 >= 8 ? 8 : P0 >= 4 ? 4 : P0 >= 2 ? 2 : 1;
-  static constexpr int PC_EPI = PC;
+  static constexpr int PC_EPI = PC;  // (four-row tiles for the 128-sample vector epilogue measured slower)
   // persistent variant (one CTA per SM, stages its inputs in shared memory): 384-thread budget, half the rows
   static constexpr int PP0 = 384 / (C * TPP);
   static constexpr int PC_PIPE0 = PP0 >= 32 ? 32 : PP0 >= 16 ? 16 : PP0 >= 8 ? 8 : PP0 >= 4 ? 4 : PP0 >= 2 ? 2 : 1;

@@ -86,6 +86,23 @@ class MixedSolution:
         self.outer_residues = []
         self.inner_iterations = []
 
+    def tune(self, iters: int = 10, candidates=None) -> dict:
+        """Choose the inner iteration's kernel variant with the autotuner.  The inner solves start from zero sources
+        (the defects are written later), so the trials run on this problem's own sources s'0 cast to complex64;
+        the inner sources and state are restored afterwards."""
+        from . import autotune
+        eng = self.inner.engine
+        saved_src = eng.sources.clone()
+        saved_state = eng.state.clone()
+        try:
+            eng.sources.copy_(self.src64.to(eng.sources.dtype))
+            eng._mark_zero_sources()
+            kw = {} if candidates is None else {'candidates': tuple(candidates)}
+            return autotune.tune(eng, iters=iters, use_cache=False, **kw)
+        finally:
+            eng.sources.copy_(saved_src)
+            eng.state.copy_(saved_state)
+
     def _xnorms(self) -> np.ndarray:
         """FP64 norms of every right-hand side's x, read back once (the launches queue on one stream and share the
         plan's scratch in order)."""
