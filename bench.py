@@ -293,7 +293,7 @@ def bench_ours(args, wl, rank, world, local, pg):
             'unit_of_launch': f'one iteration = {launches_per_iter} pass kernels (CUDA graph chunks of {chunk})',
             'algorithmic_bytes': alg, 'bytes_per_voxel': alg / nvox}
     sol._engine.close()
-    e2e = e2e_solve(wl, dtype) if rank == 0 and not args.no_e2e else None
+    e2e = e2e_solve(wl, dtype, tuned['variant'] if tuned else None) if rank == 0 and not args.no_e2e else None
     # the GPU measurements run before the host baseline, whose FFT worker threads would compete with the host side
     # of the timed GPU solves
     secondary = run_secondary(args) if rank == 0 and args.secondary != 'none' else None
@@ -675,21 +675,23 @@ def fused_epilogue(wl, variant=0) -> bool:
     return iso or int(wl['shape'][-1]) == 192
 
 
-def e2e_solve(wl, dtype):
+def e2e_solve(wl, dtype, variant=None):
     """One full solve to the workload's residue through the public API from host arrays (host->device copies of
-    chi, source and initial field, device->host copy of the solution).  A first, untimed solve captures the
-    iteration graphs."""
+    chi and source, the field started at zero on the device as the reference's Solution starts it, device->host
+    copy of the solution), on the kernel variant ``variant`` (the autotuner's choice for this problem class; None:
+    the plan's default).  A first, untimed solve captures the iteration graphs."""
     import torch
-    from macromax_b200 import Bound, Grid, Solution
+    from macromax_b200 import Bound, Grid, Solution, autotune
     grid = Grid(shape=wl['shape'], step=wl['step'])
     bound = Bound(grid, thickness=wl['bound_thickness'])
     sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
                    source_distribution=wl['source'], bound=bound, dtype=dtype)
     eng = sol._engine
+    if variant is not None:
+        autotune.set_variant(eng, int(variant))
     chi_host = eng.chi.cpu().numpy()
     src_host = eng.sources.cpu().numpy()
-    e0 = np.zeros((eng.ncomp, *wl['shape']), dtype=dtype)
-    pin = [torch.from_numpy(a).pin_memory() for a in (chi_host, src_host, e0)]
+    pin = [torch.from_numpy(a).pin_memory() for a in (chi_host, src_host)]
     out_pin = torch.empty((eng.ncomp, eng.N), dtype=eng.torch_dtype, pin_memory=True)  # the result's host buffer
     result = None
     for timed in (False, True):
@@ -697,7 +699,8 @@ def e2e_solve(wl, dtype):
         t0 = time.perf_counter()
         eng.chi.copy_(pin[0], non_blocking=True)
         eng.sources.copy_(pin[1], non_blocking=True)
-        eng.set_fields(pin[2])
+        eng.fields.zero_()
+        eng.reset_update_norm()
         eng.reset_alpha()
         st = eng.run(float(wl['rtol']), float(wl['maxiter']))
         out_pin.copy_(eng.current(st)[0])
@@ -709,7 +712,7 @@ def e2e_solve(wl, dtype):
         if timed:
             result = {'value': eng.N * iters / dt, 'unit': UNIT, 'h2d_bytes_per_step': h2d,
                       'd2h_bytes_per_step': int(out.nbytes), 'iterations': iters, 'seconds': dt,
-                      'residue': float(st['residue'][0]),
+                      'residue': float(st['residue'][0]), 'kernel_variant': autotune.get_variant(eng),
                       'step': f"one solve to residue {wl['rtol']} from host arrays (time to residual)"}
     sol._engine.close()
     # time to residual including the set-up, as a user runs it: Solution from host arrays (host FP64 preconditioner
@@ -719,6 +722,8 @@ def e2e_solve(wl, dtype):
         t0 = time.perf_counter()
         sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
                        source_distribution=wl['source'], bound=bound, dtype=dtype)
+        if variant is not None:
+            autotune.set_variant(sol._engine, int(variant))
         sol.solve(None, rtol=float(wl['rtol']), maxiter=float(wl['maxiter']))
         E = sol.E
         dt = time.perf_counter() - t0

@@ -262,8 +262,15 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 #ifndef MMX_REG_MIN_BLOCKS
 #define MMX_REG_MIN_BLOCKS 2
 #endif
+// One-component passes of up to 128 samples (128-thread CTAs: scalar fields, and the component-split FFT-only passes
+// of vector fields) are compiled for seven CTAs per SM (72 registers): 115.8 against 116.3 us per 128^3 vector
+// iteration and 49.4 against 50.8 us per 128^3 scalar iteration with the unbounded 80-register build; eight CTAs
+// (64 registers, spills) were slower.
+template <int C, int N> struct RegMinBlocks {
+  static constexpr int value = (C == 1 && N <= 128) ? 896 / RegThreads<C, N>::value : MMX_REG_MIN_BLOCKS;
+};
 template <int C, int OPS, int N>
-__global__ void __launch_bounds__(RegThreads<C, N>::value, MMX_REG_MIN_BLOCKS) k_reg_pass(IterArgs<float> a) {
+__global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::value)) k_reg_pass(IterArgs<float> a) {
   constexpr int P = kRegP;
   constexpr int THREADS = RegThreads<C, N>::value;
   extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
