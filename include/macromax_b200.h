@@ -128,7 +128,8 @@ int mmx_iterate(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kin
 int mmx_iterate_graph(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
                       mmx_rhs_state* state, int niter, void* stream);
 
-/* Capture (and cache) the graph that mmx_iterate_graph would launch, without launching it. */
+/* Capture (and cache) the graph that mmx_iterate_graph would launch, without launching it; the graph is uploaded to
+ * the device (on the legacy default stream, synchronously), so that its first launch pays no upload either. */
 int mmx_iterate_graph_prepare(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
                               mmx_rhs_state* state, int niter);
 

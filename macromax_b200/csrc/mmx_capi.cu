@@ -1354,8 +1354,15 @@ int iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E
   if (!exec) {
     const int rc = capture_multi(n, plans, E0, E1, chi, chi_kind, src, state, niter, &exec);
     if (rc != MMX_OK) return rc;
-    std::lock_guard<std::mutex> lock(g_graph_mutex);
-    g_graphs.push_back(GraphEntry{key, exec});
+    {
+      std::lock_guard<std::mutex> lock(g_graph_mutex);
+      g_graphs.push_back(GraphEntry{key, exec});
+    }
+    if (!launch) {
+      // a prepared graph is also uploaded now, so that its first launch does not pay for the upload
+      MMX_CUDA(cudaGraphUpload(exec, (cudaStream_t)0));
+      MMX_CUDA(cudaStreamSynchronize((cudaStream_t)0));
+    }
   }
   if (launch) MMX_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
   return MMX_OK;
