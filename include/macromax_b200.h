@@ -129,9 +129,23 @@ int mmx_iterate_graph(mmx_plan* plan, void* E0, void* E1, const void* chi, int c
                       mmx_rhs_state* state, int niter, void* stream);
 
 /* Capture (and cache) the graph that mmx_iterate_graph would launch, without launching it; the graph is uploaded to
- * the device (on the legacy default stream, synchronously), so that its first launch pays no upload either. */
+ * the device (on the legacy default stream, synchronously), so that its first launch pays no upload either.  Where
+ * mmx_iterate_graph_continue would start its chunk with the middle passes now, that graph is captured too. */
 int mmx_iterate_graph_prepare(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
                               mmx_rhs_state* state, int niter);
+
+/*
+ * mmx_iterate_graph for the next chunk of the same solve.  The caller guarantees that nothing has written the
+ * fields, chi, the sources or the states since the previous iteration call on this plan with the same buffers (as
+ * between the chunks of Solution.solve, solver.py:1049-1098, which only read the state).  When that call ran the
+ * fused-epilogue schedule (MMX_VARIANT_FUSED_EPILOGUE), its last pass left this chunk's first pass -- chi E + s'
+ * of the current field, transformed along the contiguous axis -- in the plan's work buffer, so the chunk starts
+ * with the middle passes instead of recomputing it; the iterates are those of one longer mmx_iterate_graph call.
+ * Otherwise (another plan call came between, the variant changed, other buffers, the plain schedule) it is
+ * mmx_iterate_graph.  No counterpart in the reference, whose solve runs every iteration from the field.
+ */
+int mmx_iterate_graph_continue(mmx_plan* plan, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
+                               mmx_rhs_state* state, int niter, void* stream);
 
 /*
  * `niter` iterations of n independent problems (plans of possibly different grid shapes, e.g. an uneven batch of

@@ -49,8 +49,8 @@ assert STATE_DTYPE.itemsize == 112
 EXPORTED = ['mmx_last_error', 'mmx_version', 'mmx_plan_create', 'mmx_plan_destroy', 'mmx_plan_set_kvectors',
             'mmx_fftn', 'mmx_norm', 'mmx_iterate', 'mmx_defect', 'mmx_accumulate', 'mmx_adjoint_grad',
             'mmx_pointwise_mul', 'mmx_fftn_noalloc', 'mmx_mat3_extremes', 'mmx_iterate_graph',
-            'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_plan_set_variant', 'mmx_plan_get_variant',
-            'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby', 'mmx_chi_from_eps',
+            'mmx_iterate_multi', 'mmx_iterate_graph_prepare', 'mmx_iterate_graph_continue', 'mmx_plan_set_variant',
+            'mmx_plan_get_variant', 'mmx_scalar_sigma', 'mmx_curl_ft', 'mmx_green_ft', 'mmx_chi_mix', 'mmx_axpby', 'mmx_chi_from_eps',
             'mmx_magnetic_iterate', 'mmx_mode_scatter', 'mmx_mode_gather']
 
 _lib = None
@@ -112,6 +112,7 @@ def load(path: str | None = None):
         'mmx_mat3_extremes': (i32, [vp, vp, i64, i32, dbl, vp, vp]),
         'mmx_iterate_graph': (i32, [vp, vp, vp, vp, i32, vp, vp, i32, vp]),
         'mmx_iterate_graph_prepare': (i32, [vp, vp, vp, vp, i32, vp, vp, i32]),
+        'mmx_iterate_graph_continue': (i32, [vp, vp, vp, vp, i32, vp, vp, i32, vp]),
         'mmx_mode_scatter': (i32, [vp, vp, i64, i64, i64, i32, vp, i32, vp]),
         'mmx_mode_gather': (i32, [vp, vp, i64, i64, i64, i32, vp, i32, vp]),
         'mmx_plan_set_variant': (i32, [vp, ctypes.c_uint]),

@@ -150,6 +150,12 @@ struct mmx_plan {
   bool epro = false;           // fuse each epilogue with the next iteration's prologue
   bool tma = false;            // strided 128-sample passes staged by bulk tensor copies (k_tma_pass)
   std::vector<PassCfg> epro_passes;   // [middle passes..., EPI+PRO, repair]; the first PRO runs once per call
+  // The last iteration call on this plan whose fused epilogue left the next iteration's first pass (the prologue
+  // and the contiguous-axis forward transform of the current field) in `work`, and its buffers: E0, E1, chi, src,
+  // state.  mmx_iterate_graph_continue starts a chunk with the middle passes only when its buffers match.
+  bool cont_valid = false;
+  const void* cont_buf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int cont_kind = 0;
   // L2 residency of the work buffer (MMX_L2_PERSIST=1): the middle passes re-read T from L2
   bool l2_persist = false;
   size_t l2_window = 0;
@@ -872,9 +878,36 @@ template <class R> IterArgs<R> base_args(mmx_plan* p) {
   return a;
 }
 
+// whether run_iterations takes the fused-epilogue schedule for this plan and chi
+bool epro_runs(const mmx_plan* p, int chi_kind) {
+  if (p->prec != MMX_C64) return false;
+  const bool plane = p->plane && chi_kind == MMX_CHI_SCALAR && !p->plane_passes.empty();
+  return !plane && p->epro && epro_serves(p, chi_kind);
+}
+
+// record the buffers of an iteration call that ran to completion on the stream (or clear the record)
+void note_iteration_call(mmx_plan* p, const void* E0, const void* E1, const void* chi, int chi_kind, const void* src,
+                         const void* st) {
+  p->cont_valid = epro_runs(p, chi_kind);
+  const void* b[5] = {E0, E1, chi, src, st};
+  for (int i = 0; i < 5; ++i) p->cont_buf[i] = b[i];
+  p->cont_kind = chi_kind;
+}
+
+bool can_continue(const mmx_plan* p, const void* E0, const void* E1, const void* chi, int chi_kind, const void* src,
+                  const void* st) {
+  const void* b[5] = {E0, E1, chi, src, st};
+  if (!p->cont_valid || p->cont_kind != chi_kind || !epro_runs(p, chi_kind)) return false;
+  for (int i = 0; i < 5; ++i)
+    if (p->cont_buf[i] != b[i]) return false;
+  return true;
+}
+
+// `niter` iterations on stream s.  skip_first: the fused-epilogue schedule starts with the middle passes, because
+// the previous call's last fused epilogue (or repair pass) already wrote this chunk's first pass to the work buffer.
 template <class R>
 int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, const void* src,
-                   mmx_rhs_state* st, int niter, cudaStream_t s) {
+                   mmx_rhs_state* st, int niter, cudaStream_t s, bool skip_first = false) {
   IterArgs<R> a = base_args<R>(p);
   a.E0 = (cpx<R>*)E0;
   a.E1 = (cpx<R>*)E1;
@@ -888,9 +921,12 @@ int run_iterations(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kin
   if (epro) {
     // first prologue of the chunk, then per iteration the middle passes, the fused epilogue + next prologue and
     // the repair pass
-    a.ax = p->ax[p->iter_passes.front().axis];
-    int rc = dispatch_pass<R>(p->iter_passes.front(), a, p->ncomp, chi_kind, p->batch, s);
-    if (rc != MMX_OK) return rc;
+    int rc = MMX_OK;
+    if (!skip_first) {
+      a.ax = p->ax[p->iter_passes.front().axis];
+      rc = dispatch_pass<R>(p->iter_passes.front(), a, p->ncomp, chi_kind, p->batch, s);
+      if (rc != MMX_OK) return rc;
+    }
     for (int it = 0; it < niter; ++it) {
       for (const PassCfg& pc : p->epro_passes) {
         a.ax = p->ax[pc.axis];
@@ -1207,8 +1243,11 @@ int mmx_iterate(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind, 
   if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
   if (niter < 0) return fail(MMX_ERR_ARG, "negative iteration count");
   cudaStream_t s = (cudaStream_t)stream;
-  if (p->prec == MMX_C128) return run_iterations<double>(p, E0, E1, chi, chi_kind, src, state, niter, s);
-  return run_iterations<float>(p, E0, E1, chi, chi_kind, src, state, niter, s);
+  p->cont_valid = false;
+  const int rc = p->prec == MMX_C128 ? run_iterations<double>(p, E0, E1, chi, chi_kind, src, state, niter, s)
+                                     : run_iterations<float>(p, E0, E1, chi, chi_kind, src, state, niter, s);
+  if (rc == MMX_OK && niter > 0) note_iteration_call(p, E0, E1, chi, chi_kind, src, state);
+  return rc;
 }
 
 int mmx_defect(mmx_plan* p, const void* x, const void* chi, int chi_kind, const void* src, const mmx_rhs_state* st,
@@ -1217,6 +1256,7 @@ int mmx_defect(mmx_plan* p, const void* x, const void* chi, int chi_kind, const 
   if (p->prec != MMX_C128) return fail(MMX_ERR_ARG, "mmx_defect needs a complex128 plan");
   if (!p->kv_set) return fail(MMX_ERR_ARG, "k-vectors not set (mmx_plan_set_kvectors)");
   cudaStream_t s = (cudaStream_t)stream;
+  p->cont_valid = false;  // the defect transforms run in the work buffer
   IterArgs<double> a = base_args<double>(p);
   a.E0 = (double2*)x;
   a.E1 = (double2*)x;
@@ -1279,7 +1319,7 @@ namespace {
 // Capture `niter` iterations of every plan into one graph: the plans' passes run on forked capture streams, so
 // independent grids (e.g. batches of uneven sizes) become parallel branches of a single launch.
 int capture_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1, const void* const* chi,
-                  const int* chi_kind, const void* const* src, mmx_rhs_state* const* st, int niter,
+                  const int* chi_kind, const void* const* src, mmx_rhs_state* const* st, int niter, bool skip_first,
                   cudaGraphExec_t* out) {
   std::vector<cudaStream_t> streams(n + 1, nullptr);
   std::vector<cudaEvent_t> events(n + 1, nullptr);
@@ -1304,7 +1344,8 @@ int capture_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E
       if (p->prec == MMX_C128)
         rc = run_iterations<double>(p, E0[i], E1[i], chi[i], chi_kind[i], src[i], st[i], niter, streams[i + 1]);
       else
-        rc = run_iterations<float>(p, E0[i], E1[i], chi[i], chi_kind[i], src[i], st[i], niter, streams[i + 1]);
+        rc = run_iterations<float>(p, E0[i], E1[i], chi[i], chi_kind[i], src[i], st[i], niter, streams[i + 1],
+                                   skip_first);
       cudaEventRecord(events[i], streams[i + 1]);
       cudaStreamWaitEvent(streams[0], events[i], 0);  // join
     }
@@ -1329,9 +1370,13 @@ int capture_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E
 }  // namespace
 
 namespace {
+// Find or capture the graph of `niter` iterations of the plans and launch it on `stream` (launch = false: capture
+// and upload only).  cont (one plan): continue the previous call on these buffers -- the chunk starts with the middle
+// passes when the plan's record says the work buffer holds its first pass (can_continue); a prepared call then
+// captures that graph as well as the self-contained one.
 int iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E1, const void* const* chi,
                   const int* chi_kind, const void* const* src, mmx_rhs_state* const* state, int niter, void* stream,
-                  bool launch) {
+                  bool launch, bool cont = false) {
   if (n < 1 || !plans || !E0 || !E1 || !chi || !chi_kind || !src || !state) return fail(MMX_ERR_ARG, "NULL argument");
   if (niter < 1) return fail(MMX_ERR_ARG, "niter must be positive");
   GraphKey key;
@@ -1345,26 +1390,36 @@ int iterate_multi(int n, mmx_plan* const* plans, void* const* E0, void* const* E
     key.ints.push_back(chi_kind[i]);
   }
   key.ints.push_back(niter);
-  cudaGraphExec_t exec = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_graph_mutex);
-    for (const GraphEntry& g : g_graphs)
-      if (g.key == key) exec = g.exec;
-  }
-  if (!exec) {
-    const int rc = capture_multi(n, plans, E0, E1, chi, chi_kind, src, state, niter, &exec);
-    if (rc != MMX_OK) return rc;
+  const bool skip = cont && n == 1 && can_continue(plans[0], E0[0], E1[0], chi[0], chi_kind[0], src[0], state[0]);
+  // a prepared continuation also captures the self-contained graph; a launch takes the one that applies
+  for (int variant = (!launch && skip) ? 0 : (skip ? 1 : 0); variant <= (skip ? 1 : 0); ++variant) {
+    GraphKey k = key;
+    k.ints.push_back(variant);
+    cudaGraphExec_t exec = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_graph_mutex);
-      g_graphs.push_back(GraphEntry{key, exec});
+      for (const GraphEntry& g : g_graphs)
+        if (g.key == k) exec = g.exec;
     }
-    if (!launch) {
-      // a prepared graph is also uploaded now, so that its first launch does not pay for the upload
-      MMX_CUDA(cudaGraphUpload(exec, (cudaStream_t)0));
-      MMX_CUDA(cudaStreamSynchronize((cudaStream_t)0));
+    if (!exec) {
+      const int rc = capture_multi(n, plans, E0, E1, chi, chi_kind, src, state, niter, variant == 1, &exec);
+      if (rc != MMX_OK) return rc;
+      {
+        std::lock_guard<std::mutex> lock(g_graph_mutex);
+        g_graphs.push_back(GraphEntry{k, exec});
+      }
+      if (!launch) {
+        // a prepared graph is also uploaded now, so that its first launch does not pay for the upload
+        MMX_CUDA(cudaGraphUpload(exec, (cudaStream_t)0));
+        MMX_CUDA(cudaStreamSynchronize((cudaStream_t)0));
+      }
+    }
+    if (launch) {
+      for (int i = 0; i < n; ++i) plans[i]->cont_valid = false;
+      MMX_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
+      for (int i = 0; i < n; ++i) note_iteration_call(plans[i], E0[i], E1[i], chi[i], chi_kind[i], src[i], state[i]);
     }
   }
-  if (launch) MMX_CUDA(cudaGraphLaunch(exec, (cudaStream_t)stream));
   return MMX_OK;
 }
 }  // namespace
@@ -1382,13 +1437,19 @@ extern "C" int mmx_iterate_graph(mmx_plan* p, void* E0, void* E1, const void* ch
 
 extern "C" int mmx_iterate_graph_prepare(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind,
                                          const void* src, mmx_rhs_state* state, int niter) {
-  return iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, nullptr, false);
+  return iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, nullptr, false, true);
+}
+
+extern "C" int mmx_iterate_graph_continue(mmx_plan* p, void* E0, void* E1, const void* chi, int chi_kind,
+                                          const void* src, mmx_rhs_state* state, int niter, void* stream) {
+  return iterate_multi(1, &p, &E0, &E1, &chi, &chi_kind, &src, &state, niter, stream, true, true);
 }
 
 extern "C" int mmx_plan_set_variant(mmx_plan* p, unsigned flags) {
   if (!p) return fail(MMX_ERR_ARG, "NULL plan");
   if (flags & ~63u) return fail(MMX_ERR_ARG, "unknown variant flags");
   drop_graphs_of(p);  // captured graphs hold the previous kernels
+  p->cont_valid = false;
   p->force_generic = (flags & MMX_VARIANT_GENERIC) != 0;
   p->no_reg = (flags & MMX_VARIANT_SHARED_STAGED) != 0;
   p->pipe = (flags & MMX_VARIANT_PERSISTENT) != 0;

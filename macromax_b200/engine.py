@@ -193,10 +193,16 @@ class IterationEngine:
     # -- iteration --------------------------------------------------------------------------------------------------
     use_graphs = True  # replay captured CUDA graphs for multi-iteration chunks
 
-    def iterate(self, niter: int, stream=None):
+    def iterate(self, niter: int, stream=None, cont: bool = False):
+        """``niter`` iterations on the stream.  cont: the next chunk of the same solve -- nothing has written the
+        fields, chi, sources or states since the previous call -- so the chunk may start from the first pass that
+        the previous chunk's fused epilogue left in the work buffer (mmx_iterate_graph_continue)."""
         if niter <= 0:
             return
-        fn = 'mmx_iterate_graph' if (self.use_graphs and niter > 1) else 'mmx_iterate'
+        if self.use_graphs and niter > 1:
+            fn = 'mmx_iterate_graph_continue' if cont else 'mmx_iterate_graph'
+        else:
+            fn = 'mmx_iterate'
         nat.call(fn, self.plan.handle, _ptr(self.fields[0]), _ptr(self.fields[1]), _ptr(self.chi),
                  self.chi_kind, _ptr(self.sources), _ptr(self.state), int(niter), _stream_ptr(stream))
 
@@ -218,8 +224,10 @@ class IterationEngine:
         st['active'] = 1
         st['status'] = 0
         self.write_state(st)
+        cont = False  # the chunks after the first continue the same solve (the loop only reads the state)
         while True:
-            self.iterate(chunk)
+            self.iterate(chunk, cont=cont)
+            cont = True
             st = self.read_state()
             if not np.any(st['active']):
                 break

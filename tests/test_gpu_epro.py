@@ -130,3 +130,71 @@ def test_fused_epilogue_batched_rejections():
         i1, r1, a1, e1 = run(srcs[k:k + 1])
         assert ib[k] == i1[0] and rb[k] == r1[0] and ab[k] == a1[0]
         assert rel(eb[k], e1[0]) < 1e-6
+
+
+def test_fused_epilogue_dense_vector_source_matches_plain_schedule():
+    """A source with all three components nonzero (no source component is skipped): the fused epilogue follows the
+    plain schedule."""
+    from macromax_b200 import workloads as w
+    wl = w.spheres_3d(n=64, nb_spheres=40)
+    rng = np.random.default_rng(11)
+    src = np.asarray(wl['source']).copy()
+    src[1] = 0.3 * np.roll(src[0], 5, axis=0)
+    src[2] = (rng.standard_normal(src[2].shape) + 1j * rng.standard_normal(src[2].shape)) * 1e-2
+    wl['source'] = src
+    a, b = _solution(wl, True), _solution(wl, False)
+    a.solve(None, rtol=0, maxiter=30)
+    b.solve(None, rtol=0, maxiter=30)
+    assert a.iteration == b.iteration == 30
+    assert rel(a.E, b.E) < 2e-6
+
+
+def _chunks(wl, seq):
+    """Run chunks of iterations on one fused-epilogue solution: (niter, cont) items, or 'variant' (set the variant
+    again, which clears the plan's record of the previous call); returns the state and the current field."""
+    import torch
+    sol = _solution(wl, True)
+    eng = sol._engine
+    st = eng.read_state()
+    st['rtol'] = -1.0
+    st['maxiter'] = np.inf
+    st['active'] = 1
+    eng.write_state(st)
+    for op in seq:
+        if op == 'variant':
+            _set(eng, True)
+        else:
+            eng.iterate(op[0], cont=op[1])
+    torch.cuda.synchronize()
+    out = eng.read_state(), eng.current()[0].cpu().numpy()
+    eng.close()
+    return out
+
+
+def test_continued_chunks_equal_one_longer_chunk():
+    """mmx_iterate_graph_continue: the chunks of a solve after the first start from the first pass that the previous
+    chunk's fused epilogue left in the work buffer, so three continued chunks of 10 iterations give one 30-iteration
+    graph's fields bit for bit.  A variant change in between clears the plan's record: the next chunk then starts
+    with its own first pass, exactly like a self-contained call, and agrees with the continuation to complex64
+    rounding."""
+    wl = _cases()['spheres3d_64']()
+    sa, ea = _chunks(wl, [(10, False), (10, True), (10, True)])
+    sb, eb = _chunks(wl, [(30, False)])
+    assert int(sa['iteration'][0]) == int(sb['iteration'][0]) == 30
+    assert np.array_equal(ea, eb)
+    sc, ec = _chunks(wl, [(10, False), 'variant', (10, True)])
+    sd, ed = _chunks(wl, [(10, False), (10, False)])
+    assert int(sc['iteration'][0]) == int(sd['iteration'][0]) == 20
+    assert np.array_equal(ec, ed)
+    se, ee = _chunks(wl, [(10, False), (10, True)])
+    assert rel(ee, ed) < 1e-6
+
+
+def test_continued_chunks_with_rejections_follow_the_oracle():
+    """A gain medium whose updates are rejected: the chunk boundaries fall between rejected and accepted updates,
+    and the continued solve keeps the rejection count and the iterates of one longer call."""
+    wl = _cases()['gain2d_64']()
+    sa, ea = _chunks(wl, [(8, False)] + [(8, True)] * 4)
+    sb, eb = _chunks(wl, [(40, False)])
+    assert int(sa['rejections'][0]) == int(sb['rejections'][0]) > 0
+    assert np.array_equal(ea, eb)
