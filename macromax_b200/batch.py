@@ -158,6 +158,37 @@ class BatchSolution:
         self.engine.close()
 
 
+def solve_sharded(grid: Grid, sources, epsilon, rtol: float = 1e-6, maxiter=1e4, **kwargs) -> dict:
+    """
+    Right-hand sides of one material split over the ranks of the default process group (``torchrun``, one GPU per
+    rank, the device chosen by the caller): every rank solves its ``shard_range`` slice of ``sources``
+    [B, 1|3, *grid] in one BatchSolution on its own GPU, then the fields ``E`` [B, 1|3, *grid] and the per-source
+    ``iterations`` and ``residues`` are gathered in source order on every rank.  The solves exchange nothing (replicas);
+    the gather is the only collective.  Without a process group, or with one rank, this is one BatchSolution over all
+    sources.  ``kwargs`` go to BatchSolution (bound, vacuum_wavelength, dtype, ...).
+    """
+    from .distributed import gather_rows, shard_range, world
+    rank, size = world()
+    src = np.asarray(sources)
+    if src.ndim == grid.ndim + 1:
+        src = src[None]
+    n = int(src.shape[0])
+    a, b = shard_range(n, rank, size)
+    dtype = np.dtype(kwargs.get('dtype', np.complex64))
+    if b > a:
+        bs = BatchSolution(grid, src[a:b], epsilon, **kwargs)
+        try:
+            bs.solve(rtol, maxiter)
+            E, its, res = bs.E, bs.iterations, bs.residues
+        finally:
+            bs.close()
+    else:  # more ranks than sources: this rank contributes no rows
+        E = np.zeros((0, *src.shape[1:]), dtype=dtype)
+        its = np.zeros(0, dtype=np.int32)
+        res = np.zeros(0, dtype=np.float64)
+    return {'E': gather_rows(E, n), 'iterations': gather_rows(its, n), 'residues': gather_rows(res, n)}
+
+
 class UnevenBatch:
     """
     Several batches on grids of different sizes (e.g. 64 x 128^2, 32 x 256^2 and 8 x 384^2 sources) iterated by

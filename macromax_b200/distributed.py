@@ -4,7 +4,8 @@ Multi-GPU use of the solver: replicas only.
 A single grid is not sharded (that would need an all-to-all per FFT).  Right-hand sides that share a material are
 independent, so N processes (one per GPU) each solve their own contiguous slice of the sources with no data-path
 collective; the only collectives are the max-over-ranks of a timing and the final gather of the results
-(``ScatteringMatrix`` gathers its columns' detection vectors this way under ``torchrun``).
+(``ScatteringMatrix`` gathers its columns' detection vectors this way under ``torchrun``, and
+``batch.solve_sharded`` the fields of a batch of sources).
 """
 from __future__ import annotations
 

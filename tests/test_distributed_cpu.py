@@ -96,3 +96,86 @@ def test_scattering_matrix_columns_shard_over_two_gloo_ranks():
     assert [r[1][0] for r in results] == [4, 3]
     for rank, seen, equal, shape in results:
         assert equal and shape[0] == 7
+
+
+class _FakeBatch:
+    """Stands in for BatchSolution in the sharding tests: the 'solution' of source k is a fixed function of it."""
+    seen = []
+
+    def __init__(self, grid, sources, epsilon, **kwargs):
+        import numpy as np
+        self.src = np.asarray(sources)
+        _FakeBatch.seen.append(int(self.src.shape[0]))
+
+    def solve(self, rtol, maxiter):
+        return self
+
+    @property
+    def E(self):
+        return (self.src * (2.0 + 1.0j)).astype('complex64')
+
+    @property
+    def iterations(self):
+        return self.src[:, 0, 0, 0].real.astype('int32')
+
+    @property
+    def residues(self):
+        return self.src[:, 0, 0, 0].real * 0.5
+
+    def close(self):
+        pass
+
+
+def _sources(n=7):
+    import numpy as np
+    src = np.random.default_rng(5).standard_normal((n, 1, 6, 4)).astype(np.complex64)
+    src[:, 0, 0, 0] = np.arange(n)
+    return src
+
+
+def _batch_worker(rank, world, port, q):
+    import numpy as np
+    import torch.distributed as dist
+    from macromax_b200 import Grid, batch
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        batch.BatchSolution = _FakeBatch
+        src = _sources()
+        out = batch.solve_sharded(Grid(shape=(6, 4), step=0.125), src, 1.0, vacuum_wavelength=0.5)
+        ok = (np.array_equal(out['E'], (src * (2.0 + 1.0j)).astype(np.complex64))
+              and out['iterations'].tolist() == list(range(7)) and np.allclose(out['residues'], np.arange(7) * 0.5))
+        q.put((rank, list(_FakeBatch.seen), bool(ok), out['E'].shape))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batch_sources_shard_over_two_gloo_ranks():
+    """solve_sharded: each of two gloo ranks solves its shard_range slice of 7 sources (4 and 3) and both end with all
+    7 fields, iteration counts and residues in source order."""
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = 29700 + os.getpid() % 1000
+    procs = [ctx.Process(target=_batch_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    results = sorted(q.get(timeout=10) for _ in range(2))
+    assert [r[1] for r in results] == [[4], [3]]
+    for rank, seen, ok, shape in results:
+        assert ok and shape == (7, 1, 6, 4)
+
+
+def test_batch_sources_without_a_process_group_solve_all(monkeypatch):
+    import numpy as np
+    from macromax_b200 import Grid, batch
+    monkeypatch.setattr(batch, 'BatchSolution', _FakeBatch)
+    _FakeBatch.seen = []
+    src = _sources(5)
+    out = batch.solve_sharded(Grid(shape=(6, 4), step=0.125), src, 1.0, vacuum_wavelength=0.5)
+    assert _FakeBatch.seen == [5]
+    assert np.array_equal(out['E'], (src * (2.0 + 1.0j)).astype(np.complex64))
+    assert out['iterations'].tolist() == list(range(5))
