@@ -149,6 +149,7 @@ struct mmx_plan {
   std::vector<PassCfg> plane_passes;  // the 3-pass schedule used when `plane` is set and chi is isotropic
   bool epro = false;           // fuse each epilogue with the next iteration's prologue
   bool tma = false;            // strided 128-sample passes staged by bulk tensor copies (k_tma_pass)
+  bool wide_green = false;     // MMX_WIDE_GREEN=1: 16-pencil tiles for the vector axis-0 pass (tests)
   std::vector<PassCfg> epro_passes;   // [middle passes..., EPI+PRO, repair]; the first PRO runs once per call
   // The last iteration call on this plan whose fused epilogue left the next iteration's first pass (the prologue
   // and the contiguous-axis forward transform of the current field) in `work`, and its buffers: E0, E1, chi, src,
@@ -329,12 +330,38 @@ int launch_fast(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s)
   return MMX_OK;
 }
 
+// 8-pencil tiles: the axis-0 pass (forward, Green multiply, inverse) of a vector field on 128-sample pencils
+template <int C, int OPS, int N> constexpr bool kRegHalfTile = C == 3 && N == 128 && OPS == (OP_FWD | OP_G | OP_INV);
+
+template <int C, int OPS, int N, int P>
+int launch_reg_p(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
+  auto kern = k_reg_pass<C, OPS, N, P>;
+  static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
+  {
+    const int rc_ = allow_smem_once(configured, (const void*)kern, (int)kSmemCap);
+    if (rc_ != MMX_OK) return rc_;
+  }
+  a.outer = pc.outer;
+  a.inner = pc.inner;
+  a.P = P;
+  a.sP = P;
+  a.csplit = C == 1 ? pc.csplit : 0;
+  dim3 grid((unsigned)pc.tiles, (unsigned)(batch * (a.csplit > 1 ? a.csplit : 1)));
+  MMX_CUDA(launch_pass(kern, grid, dim3(RegThreads<C, N, P>::value), pc.smem, s, a));
+  MMX_CUDA(cudaGetLastError());
+  return MMX_OK;
+}
+
 template <int C, int OPS, int N>
 int launch_reg(const PassCfg& pc, IterArgs<float> a, int batch, cudaStream_t s) {
   if constexpr ((C == 3 && N > 128 && N != 192) || (C == 1 && N == 192 && OPS == (OP_FWD | OP_G | OP_INV)) ||
                 N == 384) {
     return fail(MMX_ERR_ARG, "internal: no register-staged kernel for this length");
   } else {
+    if constexpr (kRegHalfTile<C, OPS, N>) {
+      if (pc.P == 8) return launch_reg_p<C, OPS, N, 8>(pc, a, batch, s);
+    }
+    if (pc.P != kRegP) return fail(MMX_ERR_ARG, "internal: no register-staged kernel for this tile");
     auto kern = k_reg_pass<C, OPS, N>;
     static std::atomic<uint64_t> configured{0};  // devices on which the attribute is set
     {
@@ -785,6 +812,14 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
           pc.csplit = 3;
           pc.smem = ((size_t)n * kRegP + n) * sizeof(float2);
         }
+        if (!pc.tma && p->ncomp == 3 && ops == (OP_FWD | OP_G | OP_INV) && n == 128 && !p->wide_green) {
+          // The vector axis-0 pass in 8-pencil tiles (192-thread CTAs, four per SM): the same registers per thread
+          // and resident warps as 16-pencil tiles, half the work per CTA, so the pass's last partial wave drains
+          // sooner.
+          pc.P = pc.sP = 8;
+          pc.tiles = outer * inner / 8;
+          pc.smem = ((size_t)tile_rows<8>(3 * n) * 8 + n) * sizeof(float2);
+        }
       }
     }
     v.push_back(pc);
@@ -1135,6 +1170,8 @@ int mmx_plan_create(int ndim, const int64_t* shape, int ncomp, int batch, int pr
     p->no_reg = nr && nr[0] == '1';
     const char* pp = getenv("MMX_PIPE");
     p->pipe = pp && pp[0] == '1';
+    const char* wg = getenv("MMX_WIDE_GREEN");
+    p->wide_green = wg && wg[0] == '1';
     const char* pl = getenv("MMX_PIPE_POLL_LIMIT");
     if (pl && pl[0]) p->poll_limit = std::max(0, std::min(1 << 20, atoi(pl)));
     const char* lp = getenv("MMX_L2_PERSIST");

@@ -28,15 +28,26 @@ constexpr int kRegP = 16;
 template <int N> struct GreenPlan { using type = typename RegPlan<N>::type; };
 template <> struct GreenPlan<192> { using type = RegPlanList<3, 8, 8>; };
 
-template <int C, int N> struct RegThreads {
-  static constexpr int value = C * kRegP * RegPlan<N>::TPP;
+template <int C, int N, int P = kRegP> struct RegThreads {
+  static constexpr int value = C * P * RegPlan<N>::TPP;
 };
 
+// Shared-memory word of row r (= c N + j) and pencil pl in a tile of P pencils.  A 16-pencil row is one 128-byte
+// sweep of the banks, so the two rows a warp touches in one access never conflict.  An 8-pencil row is half of one,
+// and the four rows of a warp's access are consecutive (stage inputs), 8 apart (the fused Green stage's outputs) or
+// 16 apart (a radix-16 stage's outputs): one row of padding after every 16 puts two of them on each half of the
+// banks in all three cases.
+template <int P> __device__ __forceinline__ int tidx(int r, int pl) {
+  if constexpr (P == 16) return r * P + pl;
+  else return (r + (r >> 4)) * P + pl;
+}
+// rows of shared memory that `rows` tile rows take, padding included
+template <int P> __host__ __device__ constexpr int tile_rows(int rows) { return P == 16 ? rows : rows + rows / 16; }
+
 // one stage; SRC/DST: 0 = shared memory, 1 = global memory (tile-relative, row stride jstride words)
-template <int DIR, int N, int C, int RAD, int L, bool FROM_G, bool TO_G>
+template <int DIR, int N, int C, int RAD, int L, bool FROM_G, bool TO_G, int P = kRegP>
 __device__ __forceinline__ void rstage(float2* __restrict__ sm, const float2* __restrict__ tw, const float2* gsrc,
                                        float2* gdst, int64_t jstride, int64_t cstride) {
-  constexpr int P = kRegP;
   constexpr int TPP = RegPlan<N>::TPP;
   constexpr int T = N / RAD;
   constexpr int NBT = T / TPP;
@@ -56,7 +67,7 @@ __device__ __forceinline__ void rstage(float2* __restrict__ sm, const float2* __
     for (int q = 0; q < RAD; ++q) {
       const int j = i + q * T;
       if constexpr (FROM_G) u[m][q] = gsrc[c * cstride + (int64_t)j * jstride + pl];
-      else u[m][q] = sm[(c * N + j) * P + pl];
+      else u[m][q] = sm[tidx<P>(c * N + j, pl)];
     }
     if constexpr (L > 1) {
 #pragma unroll
@@ -78,25 +89,25 @@ __device__ __forceinline__ void rstage(float2* __restrict__ sm, const float2* __
     for (int q = 0; q < RAD; ++q) {
       const int j = d0 + q * L;
       if constexpr (TO_G) gdst[c * cstride + (int64_t)j * jstride + pl] = u[m][q];
-      else sm[(c * N + j) * P + pl] = u[m][q];
+      else sm[tidx<P>(c * N + j, pl)] = u[m][q];
     }
   }
   if constexpr (!TO_G) __syncthreads();
 }
 
 // all stages of one transform; FIRST_G: first stage reads global; LAST_G: last stage writes global
-template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, int R0, int... Rs>
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int P, int L, int R0, int... Rs>
 __device__ __forceinline__ void rstages(float2* sm, const float2* tw, const float2* gsrc, float2* gdst, int64_t js,
                                         int64_t cs) {
   constexpr bool last = sizeof...(Rs) == 0;
-  rstage<DIR, N, C, R0, L, FIRST_G, LAST_G && last>(sm, tw, gsrc, gdst, js, cs);
-  if constexpr (!last) rstages<DIR, N, C, false, LAST_G, L * R0, Rs...>(sm, tw, gsrc, gdst, js, cs);
+  rstage<DIR, N, C, R0, L, FIRST_G, LAST_G && last, P>(sm, tw, gsrc, gdst, js, cs);
+  if constexpr (!last) rstages<DIR, N, C, false, LAST_G, P, L * R0, Rs...>(sm, tw, gsrc, gdst, js, cs);
 }
 
-template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int... Rs>
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int P = kRegP, int... Rs>
 __device__ __forceinline__ void rfft(float2* sm, const float2* tw, const float2* gsrc, float2* gdst, int64_t js,
                                      int64_t cs, RegPlanList<Rs...>) {
-  rstages<DIR, N, C, FIRST_G, LAST_G, 1, Rs...>(sm, tw, gsrc, gdst, js, cs);
+  rstages<DIR, N, C, FIRST_G, LAST_G, P, 1, Rs...>(sm, tw, gsrc, gdst, js, cs);
 }
 
 // Radix-plan list algebra: concatenation, reversal, all-but-last and last.
@@ -122,18 +133,18 @@ template <int R0, int R1, int... Rs> struct PlanLast<RegPlanList<R0, R1, Rs...>>
 
 // The stages of `List` in order, the first one at span L (FIRST_G: it reads global memory; LAST_G: the last one
 // writes global memory).
-template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, class List> struct RChain;
-template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L>
-struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<>> {
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, class List, int P = kRegP> struct RChain;
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, int P>
+struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<>, P> {
   static __device__ __forceinline__ void run(float2*, const float2*, const float2*, float2*, int64_t, int64_t) {}
 };
-template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, int R0, int... Rs>
-struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<R0, Rs...>> {
+template <int DIR, int N, int C, bool FIRST_G, bool LAST_G, int L, int R0, int... Rs, int P>
+struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<R0, Rs...>, P> {
   static __device__ __forceinline__ void run(float2* sm, const float2* tw, const float2* gsrc, float2* gdst,
                                              int64_t js, int64_t cs) {
     constexpr bool last = sizeof...(Rs) == 0;
-    rstage<DIR, N, C, R0, L, FIRST_G, LAST_G && last>(sm, tw, gsrc, gdst, js, cs);
-    RChain<DIR, N, C, false, LAST_G, L * R0, RegPlanList<Rs...>>::run(sm, tw, gsrc, gdst, js, cs);
+    rstage<DIR, N, C, R0, L, FIRST_G, LAST_G && last, P>(sm, tw, gsrc, gdst, js, cs);
+    RChain<DIR, N, C, false, LAST_G, L * R0, RegPlanList<Rs...>, P>::run(sm, tw, gsrc, gdst, js, cs);
   }
 };
 
@@ -142,10 +153,10 @@ struct RChain<DIR, N, C, FIRST_G, LAST_G, L, RegPlanList<R0, Rs...>> {
 // are exactly the inputs of butterfly i of the first inverse stage when the inverse runs the radix plan in reverse
 // order; so the spectrum never goes back to shared memory between the two transforms.
 //   g(k) = -i a_i / (|k|^2 - a) / N  (solver.py:566-568, with the 1/N of the inverse transform)
-template <int N, int R>
+template <int N, int R, int P = kRegP>
 __device__ __forceinline__ void green_fused_scalar(float2* sm, const float2* tw, const float* sk0, const float* sk1,
                                                    const float* sk2, float ar, float ai, float ai2s, float ais) {
-  constexpr int P = kRegP, TPP = RegPlan<N>::TPP, T = N / R, NB = T / TPP;
+  constexpr int TPP = RegPlan<N>::TPP, T = N / R, NB = T / TPP;
   static_assert(NB >= 1 && T % TPP == 0, "stage does not split evenly over the threads");
   // The stage reads positions i + q T and writes i R + q of the same pencil, so all of a pencil's reads precede its
   // writes.  At 512 samples it runs in NB rounds over P / NB pencils each, one butterfly per thread and round, which
@@ -165,7 +176,7 @@ __device__ __forceinline__ void green_fused_scalar(float2* sm, const float2* tw,
     for (int m = 0; m < NBR; ++m) {
       const int i = ii + m * TPP * ROUNDS;
 #pragma unroll
-      for (int q = 0; q < R; ++q) u[m][q] = sm[(i + q * T) * P + pl];
+      for (int q = 0; q < R; ++q) u[m][q] = sm[tidx<P>(i + q * T, pl)];
 #pragma unroll
       for (int q = 1; q < R; ++q) u[m][q] = u[m][q] * tw[q * i];
       bfly<float, R, -1>(u[m], tw, N);
@@ -183,7 +194,7 @@ __device__ __forceinline__ void green_fused_scalar(float2* sm, const float2* tw,
     for (int m = 0; m < NBR; ++m) {
       const int i = ii + m * TPP * ROUNDS;
 #pragma unroll
-      for (int q = 0; q < R; ++q) sm[(i * R + q) * P + pl] = u[m][q];
+      for (int q = 0; q < R; ++q) sm[tidx<P>(i * R + q, pl)] = u[m][q];
     }
     __syncthreads();
   }
@@ -194,12 +205,12 @@ __device__ __forceinline__ void green_fused_scalar(float2* sm, const float2* tw,
 // the whole vector at each k:  F' = g (F - P_L F) + (i alpha_i / alpha) P_L F / N,  P_L = k k^T / |k|^2, with the
 // DC rule of the reference (P_L F = F on the grid's axes at k = 0) and no longitudinal part along absent axes.
 // The P x (N / R) items are spread over the first threads of the block; the others only join the barriers.
-template <int N, int R>
+template <int N, int R, int P = kRegP>
 __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw, const float* sk0, const float* sk1,
                                                    const float* sk2, bool dc_tile, int ndim, float ar, float ai,
                                                    float ai2s, float ais, float2 hs) {
-  constexpr int P = kRegP, T = N / R, ITEMS = P * T;
-  constexpr int THREADS = RegThreads<3, N>::value;
+  constexpr int T = N / R, ITEMS = P * T;
+  constexpr int THREADS = RegThreads<3, N, P>::value;
   static_assert(ITEMS <= THREADS, "one item per thread");
   const int tid = threadIdx.x;
   const int pl = tid % P;
@@ -213,7 +224,7 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) u[c][q] = sm[(c * N + i + q * T) * P + pl];
+      for (int q = 0; q < R; ++q) u[c][q] = sm[tidx<P>(c * N + i + q * T, pl)];
 #pragma unroll
       for (int q = 1; q < R; ++q) u[c][q] = u[c][q] * tw[q * i];
       bfly<float, R, -1>(u[c], tw, N);
@@ -251,7 +262,7 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
-      for (int q = 0; q < R; ++q) sm[(c * N + i * R + q) * P + pl] = u[c][q];
+      for (int q = 0; q < R; ++q) sm[tidx<P>(c * N + i * R + q, pl)] = u[c][q];
     }
   }
   __syncthreads();
@@ -266,16 +277,20 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 // of vector fields) are compiled for seven CTAs per SM (72 registers): 115.8 against 116.3 us per 128^3 vector
 // iteration and 49.4 against 50.8 us per 128^3 scalar iteration with the unbounded 80-register build; eight CTAs
 // (64 registers, spills) were slower.
-template <int C, int N> struct RegMinBlocks {
-  static constexpr int value = (C == 1 && N <= 128) ? 896 / RegThreads<C, N>::value : MMX_REG_MIN_BLOCKS;
+// The 8-pencil tiles of the vector axis-0 pass (192 threads) keep the 16-pencil kernel's registers per thread at
+// four CTAs per SM.
+template <int C, int N, int P = kRegP> struct RegMinBlocks {
+  static constexpr int value = (C == 1 && N <= 128) ? 896 / RegThreads<C, N, P>::value
+                               : P == 8                ? 768 / RegThreads<C, N, P>::value
+                                                       : MMX_REG_MIN_BLOCKS;
 };
-template <int C, int OPS, int N>
-__global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::value)) k_reg_pass(IterArgs<float> a) {
-  constexpr int P = kRegP;
-  constexpr int THREADS = RegThreads<C, N>::value;
+template <int C, int OPS, int N, int P = kRegP>
+__global__ void __launch_bounds__(RegThreads<C, N, P>::value, (RegMinBlocks<C, N, P>::value))
+    k_reg_pass(IterArgs<float> a) {
+  constexpr int THREADS = RegThreads<C, N, P>::value;
   extern __shared__ __align__(16) unsigned char mmx_smem_raw[];
   float2* sm = reinterpret_cast<float2*>(mmx_smem_raw);
-  float2* smtw = sm + C * N * P;
+  float2* smtw = sm + tile_rows<P>(C * N) * P;
   // component split (one-component kernel on a vector field): blockIdx.y = RHS * csplit + component
   const bool split = C == 1 && a.csplit > 1;
   const int b = split ? (int)blockIdx.y / a.csplit : (int)blockIdx.y;
@@ -295,9 +310,9 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::
   __syncthreads();
   using Plan = typename RegPlan<N>::type;
   if constexpr (OPS == OP_FWD) {
-    rfft<-1, N, C, true, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
+    rfft<-1, N, C, true, true, P>(sm, smtw, tile, tile, inner, a.N, Plan{});
   } else if constexpr (OPS == OP_INV) {
-    rfft<+1, N, C, true, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
+    rfft<+1, N, C, true, true, P>(sm, smtw, tile, tile, inner, a.N, Plan{});
   } else {
     __shared__ float sk1[P], sk2[P], sk0[N];
     const ChiCoef<float> cc = chi_coef<float>(st);
@@ -322,10 +337,10 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::
       // (the forward chain's first stage reads global memory only; its closing barrier publishes the tables)
       using Init = typename PlanInit<Plan>::type;
       constexpr int RL = PlanLast<Plan>::value;
-      RChain<-1, N, 1, true, false, 1, Init>::run(sm, smtw, tile, tile, inner, a.N);
+      RChain<-1, N, 1, true, false, 1, Init, P>::run(sm, smtw, tile, tile, inner, a.N);
       const float ar = cc.alpha_re, ai = cc.alpha_im;
-      green_fused_scalar<N, RL>(sm, smtw, sk0, sk1, sk2, ar, ai, ai * ai * a.inv_total, -ai * a.inv_total);
-      RChain<+1, N, 1, false, true, RL, typename PlanReverse<Init>::type>::run(sm, smtw, tile, tile, inner, a.N);
+      green_fused_scalar<N, RL, P>(sm, smtw, sk0, sk1, sk2, ar, ai, ai * ai * a.inv_total, -ai * a.inv_total);
+      RChain<+1, N, 1, false, true, RL, typename PlanReverse<Init>::type, P>::run(sm, smtw, tile, tile, inner, a.N);
       return;
     } else if constexpr (C == 3 && (N == 128 || N == 192)) {
       // vector field: the same fused schedule with the dyadic Green multiply (all three components per item)
@@ -347,16 +362,17 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::
       using GPlan = typename GreenPlan<N>::type;
       using Init = typename PlanInit<GPlan>::type;
       constexpr int RL = PlanLast<GPlan>::value;
-      RChain<-1, N, 3, true, false, 1, Init>::run(sm, smtw, tile, tile, inner, a.N);
+      RChain<-1, N, 3, true, false, 1, Init, P>::run(sm, smtw, tile, tile, inner, a.N);
       const float ar = cc.alpha_re, ai = cc.alpha_im;
       const float2 hs = divc(make_float2(0.f, ai), make_float2(ar, ai)) * a.inv_total;
-      green_fused_vector<N, RL>(sm, smtw, sk0, sk1, sk2, in0 == 0, a.ndim, ar, ai, ai * ai * a.inv_total,
-                                -ai * a.inv_total, hs);
-      RChain<+1, N, 3, false, true, RL, typename PlanReverse<Init>::type>::run(sm, smtw, tile, tile, inner, a.N);
+      green_fused_vector<N, RL, P>(sm, smtw, sk0, sk1, sk2, in0 == 0, a.ndim, ar, ai, ai * ai * a.inv_total,
+                                   -ai * a.inv_total, hs);
+      RChain<+1, N, 3, false, true, RL, typename PlanReverse<Init>::type, P>::run(sm, smtw, tile, tile, inner,
+                                                                                   a.N);
       return;
     }
     // forward transform into shared memory, Green multiply, inverse transform back to global memory
-    rfft<-1, N, C, true, false>(sm, smtw, tile, tile, inner, a.N, Plan{});
+    rfft<-1, N, C, true, false, P>(sm, smtw, tile, tile, inner, a.N, Plan{});
     if (tid < P) {
       const int64_t p = in0 + tid;
       float k1 = 0.f, k2 = 0.f;
@@ -385,12 +401,12 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::
       const float inv = __fdividef(1.f, fmaf(dr, dr, ai * ai));
       const float2 g = make_float2(ai2s * inv, ais * dr * inv);  // -i a_i / (|k|^2 - a) / N
       if constexpr (C == 1) {
-        sm[j * P + pl] = sm[j * P + pl] * g;
+        sm[tidx<P>(j, pl)] = sm[tidx<P>(j, pl)] * g;
       } else {
         float2 F[3], PL[3];
         const float kv[3] = {k0, k1, k2};
 #pragma unroll
-        for (int c = 0; c < 3; ++c) F[c] = sm[(c * N + j) * P + pl];
+        for (int c = 0; c < 3; ++c) F[c] = sm[tidx<P>(c * N + j, pl)];
         if (j == 0 && in0 + pl == 0) {
 #pragma unroll
           for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? F[c] : make_float2(0.f, 0.f);
@@ -404,11 +420,11 @@ __global__ void __launch_bounds__(RegThreads<C, N>::value, (RegMinBlocks<C, N>::
           for (int c = 0; c < 3; ++c) PL[c] = c < a.ndim ? kv[c] * proj : make_float2(0.f, 0.f);
         }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) sm[(c * N + j) * P + pl] = g * (F[c] - PL[c]) + hs * PL[c];
+        for (int c = 0; c < 3; ++c) sm[tidx<P>(c * N + j, pl)] = g * (F[c] - PL[c]) + hs * PL[c];
       }
     }
     __syncthreads();
-    rfft<+1, N, C, false, true>(sm, smtw, tile, tile, inner, a.N, Plan{});
+    rfft<+1, N, C, false, true, P>(sm, smtw, tile, tile, inner, a.N, Plan{});
   }
 }
 

@@ -99,3 +99,21 @@ def test_batch_fast_path_vector_128():
                        bound=bound, dtype=np.complex64)
         sol.solve(None, rtol=0, maxiter=12)
         assert rel(bs.E[b], sol.E) < 1e-6
+
+
+def test_solve_sharded_on_one_rank_is_the_batch_solve():
+    """batch.solve_sharded without a process group: one BatchSolution over all sources, the same fields and counts."""
+    from macromax_b200 import Bound, Grid
+    from macromax_b200.batch import BatchSolution, solve_sharded
+    z = load_golden('disks2d_64_c128')
+    grid = Grid(shape=tuple(int(s) for s in z['shape']), step=float(z['step']))
+    bound = Bound(grid, thickness=float(z['bound_thickness']))
+    srcs = _sources(z['source'], 3, seed=4)
+    kw = dict(bound=bound, vacuum_wavelength=float(z['wavelength']), dtype=np.complex128)
+    out = solve_sharded(grid, srcs, z['epsilon'], rtol=1e-6, maxiter=400, **kw)
+    bs = BatchSolution(grid, srcs, z['epsilon'], **kw)
+    bs.solve(rtol=1e-6, maxiter=400)
+    assert out['iterations'].tolist() == bs.iterations.tolist()
+    assert np.array_equal(out['E'], bs.E)
+    assert np.allclose(out['residues'], bs.residues, rtol=0, atol=0)
+    bs.close()

@@ -175,3 +175,24 @@ def test_persistent_pipeline_wait_limit_raises_timeout_and_keeps_fields_exact():
     assert int(single._engine.read_state()['status'][0]) == 0
     assert pipe.iteration == single.iteration == 6
     assert np.array_equal(pipe.E, single.E)
+
+
+@pytest.mark.parametrize('shape', [(128, 64, 48), (128, 32, 128), (128, 48)])
+def test_axis0_green_pass_8_and_16_pencil_tiles_agree_exactly(shape):
+    """The vector axis-0 pass (forward FFT, dyadic Green multiply, inverse FFT along 128-sample pencils) runs in
+    8-pencil tiles by default and in 16-pencil tiles with MMX_WIDE_GREEN=1.  Every pencil goes through the same
+    arithmetic in both, so the fields agree bit for bit (the DC pencil's tile included, on 3D and 2D grids)."""
+    from macromax_b200 import workloads as w
+    base = w.spheres_3d(n=48, nb_spheres=20)
+    rng = np.random.default_rng(3)
+    eps = 1.0 + 0.8 * rng.uniform(size=shape) + 0.02j
+    src = np.zeros((3, *shape), dtype=np.complex128)
+    src[0][(slice(None),) * (len(shape) - 1) + (shape[-1] // 3,)] = 1.0
+    src[2][(shape[0] // 2,) + (slice(None),) * (len(shape) - 1)] = 0.5j
+    wl = {**base, 'shape': shape, 'epsilon': eps, 'source': src, 'bound_thickness': 4 * base['step']}
+    eight = _solution_env(wl, {'MMX_WIDE_GREEN': '0'})
+    sixteen = _solution_env(wl, {'MMX_WIDE_GREEN': '1'})
+    eight.solve(None, rtol=0, maxiter=12)
+    sixteen.solve(None, rtol=0, maxiter=12)
+    assert eight.iteration == sixteen.iteration == 12
+    assert np.array_equal(eight.E, sixteen.E)
