@@ -408,7 +408,8 @@ def run_secondary(args):
       - the standalone transform mmx_fftn (BackEnd.ft) of three 128^3 complex64 fields;
       - batched mixed precision (2D scalar slab, 512^2 grid, 256 plane-wave sources) to residue 1e-8, with the error
         of 8 seeded sources against FP64 solutions, against the plain complex64 per-source loop (one Solution per
-        source for all 256 sources, to 1e-5: single precision cannot reach 1e-8); and the uneven batch
+        source for all 256 sources, to 1e-5: single precision cannot reach 1e-8), each on the kernel variant the
+        autotuner picks for it (chosen before the timed solves); and the uneven batch
         64 x 128^2 + 32 x 256^2 + 8 x 384^2 to 1e-8;
       - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve in complex64 to 1e-6,
         and in mixed precision to 1e-10, each gradient's error against the same gradient from FP64 solves.
@@ -423,6 +424,9 @@ def run_secondary(args):
     bound = Bound(grid, thickness=wl['bound_thickness'])
     t0 = time.perf_counter()
     ms = MixedSolution(grid, wl['source'], wl['epsilon'], bound=bound, vacuum_wavelength=wl['wavelength'])
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    tuned_batch = ms.tune()  # the inner iteration's kernel variant, chosen before the timed solve
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     ms.solve(rtol=1e-8, inner_rtol=MIXED_INNER_RTOL)
@@ -446,12 +450,18 @@ def run_secondary(args):
         errs.append(float(np.linalg.norm((x_sample[k] - ref).ravel()) / np.linalg.norm(ref.ravel())))
         sol._engine.close()
     # the plain complex64 loop: one Solution per source, every one of the 256 sources, to 1e-5 (single precision
-    # alone does not reach 1e-8)
+    # alone does not reach 1e-8), on the kernel variant the autotuner picks for one source of this problem
+    from macromax_b200 import autotune
     seq = 0.0
     its = 0
+    tuned_single = None
     for b in range(256):
         sol = Solution(grid, vacuum_wavelength=wl['wavelength'], epsilon=wl['epsilon'],
                        source_distribution=wl['source'][b], bound=bound, dtype=np.complex64)
+        if tuned_single is None:  # (the trials restore the fields and the state)
+            tuned_single = autotune.tune(sol._engine, iters=10, use_cache=False)
+        else:
+            autotune.set_variant(sol._engine, tuned_single['variant'])
         torch.cuda.synchronize()
         a = time.perf_counter()
         sol.solve(None, rtol=1e-5, maxiter=100000)
@@ -466,6 +476,7 @@ def run_secondary(args):
                                    'reference': 'device complex128 iteration to residue 1e-12'},
         'plain_c64_loop_to_1e-5_s (all 256 sources)': seq, 'plain_iterations_per_source': its / 256,
         'speedup_vs_plain_loop': seq / mixed_s,
+        'kernel_variant': {'batched_inner': tuned_batch, 'plain_loop': tuned_single},
         'voxel_iterations_per_s': 256 * 512 * 512 * inner / mixed_s}
     torch.cuda.empty_cache()
     # the uneven batch of the same material class: 64 x 128^2, 32 x 256^2 and 8 x 384^2 sources to 1e-8, all

@@ -170,8 +170,10 @@ class MixedSolution:
             if self._outer_begin(rtol):
                 break
             chunk = 8
+            cont = False  # the inner solve's later chunks continue its first (the loop only reads the state)
             while True:
-                eng.iterate(chunk)
+                eng.iterate(chunk, cont=cont)
+                cont = True
                 if not np.any(eng.read_state()['active']):
                     break
                 chunk = min(2 * chunk, 64)
