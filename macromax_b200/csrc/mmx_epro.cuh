@@ -149,6 +149,16 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, 
     for (int cc2 = 0; cc2 < C; ++cc2)
       if (!source_is_zero(st, cc2)) prefetch_l2(a.src + ((int64_t)b * C + cc2) * N3 + row0, chunk);
   }
+  // the twiddle table is constant: loaded into registers before the wait, stored to shared memory after it with no
+  // barrier of its own (the first inverse stage uses constant-coefficient butterflies only; its closing barrier
+  // publishes the table)
+  constexpr int TWR = (N + THREADS - 1) / THREADS;
+  static_assert(const_coef_radix(PA::R_first), "the first stage must not read the twiddle table");
+  const float2* twg = (const float2*)a.ax.tw;
+  float2 twv[TWR];
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if ((int)threadIdx.x + k * THREADS < N) twv[k] = twg[threadIdx.x + k * THREADS];
   pdl_wait();
   pdl_trigger();
   if (!st->active) return;
@@ -166,9 +176,9 @@ __global__ void __launch_bounds__(RegC<C, N, PC>::THREADS, (EproMinBlocks<C, N, 
 #pragma unroll
     for (int cc2 = 0; cc2 < C; ++cc2) prefetch_l2(Ecur + fbase + cc2 * N3 + row0, chunk);
   }
-  const float2* twg = (const float2*)a.ax.tw;
-  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
-  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if (tid + k * THREADS < N) smtw[tid + k * THREADS] = twv[k];
 
   // inverse transform of T: first stage from global memory, middle stages in shared memory
   float2* __restrict__ trow = a.T + fbase + c * N3 + rowbase;
@@ -329,6 +339,16 @@ __global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_epro
   const int b = blockIdx.y;
   const mmx_rhs_state* st = a.st + b;
   const int64_t N3 = a.N;
+  // the twiddle table is constant: loaded into registers before the wait, stored to shared memory after it with no
+  // barrier of its own (the first inverse stage's butterflies use constant coefficients; its closing barrier
+  // publishes the table)
+  constexpr int TWR = (N + THREADS - 1) / THREADS;
+  static_assert(const_coef_radix(RAD), "the first stage must not read the twiddle table");
+  const float2* twg = (const float2*)a.ax.tw;
+  float2 twv[TWR];
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if ((int)threadIdx.x + k * THREADS < N) twv[k] = twg[threadIdx.x + k * THREADS];
   pdl_wait();
   pdl_trigger();
   if (!st->active) return;
@@ -343,9 +363,9 @@ __global__ void __launch_bounds__(RegC<3, N, PC_>::THREADS, 4) k_regc_aniso_epro
   const int cur = st->cur;
   const float2* __restrict__ Ecur = cur ? a.E1 : a.E0;
   float2* __restrict__ Eoth = cur ? a.E0 : a.E1;
-  const float2* twg = (const float2*)a.ax.tw;
-  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
-  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if (tid + k * THREADS < N) smtw[tid + k * THREADS] = twv[k];
   const int64_t ibase = ((int64_t)blockIdx.x * PC + irow) * N;  // voxel of sample 0 of the item's row
   const float2* __restrict__ eI = Ecur + fbase + ibase;          // component r at eI[r N3 + sample]
   const float2* __restrict__ xI = a.chi + ibase;                 // entry k at xI[k N3 + sample]

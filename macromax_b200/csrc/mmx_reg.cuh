@@ -125,6 +125,12 @@ template <int R0> struct PlanInit<RegPlanList<R0>> { using type = RegPlanList<>;
 template <int R0, int R1, int... Rs> struct PlanInit<RegPlanList<R0, R1, Rs...>> {
   using type = typename PlanConcat<RegPlanList<R0>, typename PlanInit<RegPlanList<R1, Rs...>>::type>::type;
 };
+template <class L> struct PlanFirst;
+template <int R0, int... Rs> struct PlanFirst<RegPlanList<R0, Rs...>> { static constexpr int value = R0; };
+// radices whose butterflies use constant coefficients only (no twiddle table)
+__host__ __device__ constexpr bool const_coef_radix(int r) {
+  return r == 2 || r == 3 || r == 4 || r == 5 || r == 8 || r == 16;
+}
 template <class L> struct PlanLast;
 template <int R0> struct PlanLast<RegPlanList<R0>> { static constexpr int value = R0; };
 template <int R0, int R1, int... Rs> struct PlanLast<RegPlanList<R0, R1, Rs...>> {
@@ -296,19 +302,52 @@ __global__ void __launch_bounds__(RegThreads<C, N, P>::value, (RegMinBlocks<C, N
   const int b = split ? (int)blockIdx.y / a.csplit : (int)blockIdx.y;
   const int64_t field0 = split ? (int64_t)blockIdx.y : (int64_t)b * C;  // first component plane of the tile
   const mmx_rhs_state* st = a.st + b;
-  pdl_wait();
-  pdl_trigger();
-  if (!st->active) return;
   const int tid = threadIdx.x;
   const int64_t inner = a.inner;
   const int64_t p0 = (int64_t)blockIdx.x * P;
   const int64_t o = p0 / inner;
   const int64_t in0 = p0 - o * inner;
-  float2* tile = a.T + field0 * a.N + o * (int64_t)N * inner + in0;
+  // The constant tables -- twiddles and, for the Green passes, the k values of the tile's samples and pencils -- are
+  // loaded into registers before the pass waits for its predecessor, and stored to shared memory without a barrier
+  // of their own: the first radix stage needs none of them (span 1, constant-coefficient butterflies), and its
+  // closing barrier publishes them to the later stages.  A CTA thus waits for one round of global loads (its tile)
+  // after the state instead of three.
+  constexpr int TWR = (N + THREADS - 1) / THREADS;
+  constexpr bool kGreen = (OPS & OP_G) != 0;
   const float2* twg = (const float2*)a.ax.tw;
-  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
-  __syncthreads();
+  float2 twv[TWR];
+  float kv0[kGreen ? TWR : 1];
+  float kv1 = 0.f, kv2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if (tid + k * THREADS < N) twv[k] = twg[tid + k * THREADS];
+  if constexpr (kGreen) {
+#pragma unroll
+    for (int k = 0; k < TWR; ++k)
+      if (tid + k * THREADS < N) kv0[k] = a.kv[0][tid + k * THREADS];
+    if (tid < P) {
+      const int64_t p = in0 + tid;
+      if (a.ndim == 3) {
+        const int i1 = (int)(p / a.dims[2]);
+        const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
+        kv1 = a.kv[1][i1];
+        kv2 = a.kv[2][i2];
+      } else if (a.ndim == 2) {
+        kv1 = a.kv[1][p];
+      }
+    }
+  }
+  pdl_wait();
+  pdl_trigger();
+  if (!st->active) return;
+  float2* tile = a.T + field0 * a.N + o * (int64_t)N * inner + in0;
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if (tid + k * THREADS < N) smtw[tid + k * THREADS] = twv[k];
   using Plan = typename RegPlan<N>::type;
+  static_assert(const_coef_radix(PlanFirst<Plan>::value) &&
+                    const_coef_radix(PlanFirst<typename GreenPlan<N>::type>::value),
+                "the first stage must not read the twiddle table (it is published by that stage's barrier)");
   if constexpr (OPS == OP_FWD) {
     rfft<-1, N, C, true, true, P>(sm, smtw, tile, tile, inner, a.N, Plan{});
   } else if constexpr (OPS == OP_INV) {
@@ -320,20 +359,12 @@ __global__ void __launch_bounds__(RegThreads<C, N, P>::value, (RegMinBlocks<C, N
       // scalar field: k tables first, then the forward stages but the last, the fused last-forward / Green /
       // first-inverse stage, and the remaining inverse stages in reverse radix order
       if (tid < P) {
-        const int64_t p = in0 + tid;
-        float k1 = 0.f, k2 = 0.f;
-        if (a.ndim == 3) {
-          const int i1 = (int)(p / a.dims[2]);
-          const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
-          k1 = a.kv[1][i1];
-          k2 = a.kv[2][i2];
-        } else if (a.ndim == 2) {
-          k1 = a.kv[1][p];
-        }
-        sk1[tid] = k1;
-        sk2[tid] = k2;
+        sk1[tid] = kv1;
+        sk2[tid] = kv2;
       }
-      for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
+#pragma unroll
+      for (int k = 0; k < TWR; ++k)
+        if (tid + k * THREADS < N) sk0[tid + k * THREADS] = kv0[k];
       // (the forward chain's first stage reads global memory only; its closing barrier publishes the tables)
       using Init = typename PlanInit<Plan>::type;
       constexpr int RL = PlanLast<Plan>::value;
@@ -345,20 +376,12 @@ __global__ void __launch_bounds__(RegThreads<C, N, P>::value, (RegMinBlocks<C, N
     } else if constexpr (C == 3 && (N == 128 || N == 192)) {
       // vector field: the same fused schedule with the dyadic Green multiply (all three components per item)
       if (tid < P) {
-        const int64_t p = in0 + tid;
-        float k1 = 0.f, k2 = 0.f;
-        if (a.ndim == 3) {
-          const int i1 = (int)(p / a.dims[2]);
-          const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
-          k1 = a.kv[1][i1];
-          k2 = a.kv[2][i2];
-        } else if (a.ndim == 2) {
-          k1 = a.kv[1][p];
-        }
-        sk1[tid] = k1;
-        sk2[tid] = k2;
+        sk1[tid] = kv1;
+        sk2[tid] = kv2;
       }
-      for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
+#pragma unroll
+      for (int k = 0; k < TWR; ++k)
+        if (tid + k * THREADS < N) sk0[tid + k * THREADS] = kv0[k];
       using GPlan = typename GreenPlan<N>::type;
       using Init = typename PlanInit<GPlan>::type;
       constexpr int RL = PlanLast<GPlan>::value;
@@ -374,20 +397,12 @@ __global__ void __launch_bounds__(RegThreads<C, N, P>::value, (RegMinBlocks<C, N
     // forward transform into shared memory, Green multiply, inverse transform back to global memory
     rfft<-1, N, C, true, false, P>(sm, smtw, tile, tile, inner, a.N, Plan{});
     if (tid < P) {
-      const int64_t p = in0 + tid;
-      float k1 = 0.f, k2 = 0.f;
-      if (a.ndim == 3) {
-        const int i1 = (int)(p / a.dims[2]);
-        const int i2 = (int)(p - (int64_t)i1 * a.dims[2]);
-        k1 = a.kv[1][i1];
-        k2 = a.kv[2][i2];
-      } else if (a.ndim == 2) {
-        k1 = a.kv[1][p];
-      }
-      sk1[tid] = k1;
-      sk2[tid] = k2;
+      sk1[tid] = kv1;
+      sk2[tid] = kv2;
     }
-    for (int t = tid; t < N; t += THREADS) sk0[t] = a.kv[0][t];
+#pragma unroll
+    for (int k = 0; k < TWR; ++k)
+      if (tid + k * THREADS < N) sk0[tid + k * THREADS] = kv0[k];
     __syncthreads();
     const float ar = cc.alpha_re, ai = cc.alpha_im;
     const float2 hs = divc(make_float2(0.f, ai), make_float2(ar, ai)) * a.inv_total;
