@@ -627,6 +627,15 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
         if (!source_is_zero(st, cc2)) prefetch_l2(a.src + ((int64_t)b * C + cc2) * a.N + row0, chunk);
     }
   }
+  // the twiddle table is constant: loaded into registers before the wait, stored to shared memory after it with no
+  // barrier of its own (both first stages use constant-coefficient butterflies; their closing barriers publish it)
+  constexpr int TWR = (N + THREADS - 1) / THREADS;
+  static_assert(const_coef_radix(PA::R_first), "the first stage must not read the twiddle table");
+  const float2* twg = (const float2*)a.ax.tw;
+  float2 twv[TWR];
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if ((int)threadIdx.x + k * THREADS < N) twv[k] = twg[threadIdx.x + k * THREADS];
   pdl_wait();
   pdl_trigger();
   if (!st->active) return;
@@ -641,9 +650,9 @@ __global__ void __launch_bounds__(RegC<C, N, PC_>::THREADS, (RegCMinBlocks<C, OP
   const int cur = st->cur;
   const float2* __restrict__ Ecur = cur ? a.E1 : a.E0;
   float2* __restrict__ Eoth = cur ? a.E0 : a.E1;
-  const float2* twg = (const float2*)a.ax.tw;
-  for (int t = tid; t < N; t += THREADS) smtw[t] = twg[t];
-  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < TWR; ++k)
+    if (tid + k * THREADS < N) smtw[tid + k * THREADS] = twv[k];
 
   if constexpr (OPS == (OP_PRO | OP_FWD)) {
     // E, s' and chi of the tile's rows are contiguous chunks: prefetch them into L2 in bulk
