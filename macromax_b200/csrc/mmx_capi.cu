@@ -920,7 +920,8 @@ bool epro_runs(const mmx_plan* p, int chi_kind) {
   return !plane && p->epro && epro_serves(p, chi_kind);
 }
 
-// record the buffers of an iteration call that ran to completion on the stream (or clear the record)
+// record the buffers of an iteration call just launched on the stream (the record is cleared unless the call ran
+// the fused-epilogue schedule; later calls on the stream run after it)
 void note_iteration_call(mmx_plan* p, const void* E0, const void* E1, const void* chi, int chi_kind, const void* src,
                          const void* st) {
   p->cont_valid = epro_runs(p, chi_kind);
