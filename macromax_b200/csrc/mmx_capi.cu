@@ -813,9 +813,8 @@ std::vector<PassCfg> build_passes(const mmx_plan* p, bool defect) {
           pc.smem = ((size_t)n * kRegP + n) * sizeof(float2);
         }
         if (!pc.tma && p->ncomp == 3 && ops == (OP_FWD | OP_G | OP_INV) && n == 128 && !p->wide_green) {
-          // The vector axis-0 pass in 8-pencil tiles (192-thread CTAs, four per SM): the same registers per thread
-          // and resident warps as 16-pencil tiles, half the work per CTA, so the pass's last partial wave drains
-          // sooner.
+          // The vector axis-0 pass in 8-pencil tiles (192-thread CTAs, five per SM): half the work per CTA, so the
+          // pass's last partial wave drains sooner, and more resident warps than two 384-thread CTAs.
           pc.P = pc.sP = 8;
           pc.tiles = outer * inner / 8;
           pc.smem = ((size_t)tile_rows<8>(3 * n) * 8 + n) * sizeof(float2);

@@ -283,11 +283,11 @@ __device__ __forceinline__ void green_fused_vector(float2* sm, const float2* tw,
 // of vector fields) are compiled for seven CTAs per SM (72 registers): 115.8 against 116.3 us per 128^3 vector
 // iteration and 49.4 against 50.8 us per 128^3 scalar iteration with the unbounded 80-register build; eight CTAs
 // (64 registers, spills) were slower.
-// The 8-pencil tiles of the vector axis-0 pass (192 threads) keep the 16-pencil kernel's registers per thread at
-// four CTAs per SM.
+// The 8-pencil tiles of the vector axis-0 pass (192 threads) run five CTAs per SM at 64 registers (16 bytes of
+// spills): 109.6 against 110.7 us per 128^3 vector iteration with four CTAs at 80 registers.
 template <int C, int N, int P = kRegP> struct RegMinBlocks {
   static constexpr int value = (C == 1 && N <= 128) ? 896 / RegThreads<C, N, P>::value
-                               : P == 8                ? 768 / RegThreads<C, N, P>::value
+                               : P == 8                ? 960 / RegThreads<C, N, P>::value
                                                        : MMX_REG_MIN_BLOCKS;
 };
 template <int C, int OPS, int N, int P = kRegP>
