@@ -51,13 +51,18 @@ def _cases():
         'spheres3d_64': lambda: w.spheres_3d(n=64, nb_spheres=40),
         'design3d_64': lambda: w.design_3d(n=64),
         'disks2d_256': lambda: w.disks_2d(n=256),
+        'design3d_128': lambda: w.design_3d(n=128),
+        'slab2d_512': lambda: {**w.correlated_slab_2d(n=512, nb_modes=1),
+                               'source': w.correlated_slab_2d(n=512, nb_modes=1)['source'][0]},
         'gain2d_64': lambda: _gain_2d(64),
         'gain2d_128': lambda: _gain_2d(128, seed=3, gain=0.4),
     }
 
 
-@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256'])
+@pytest.mark.parametrize('name', ['spheres3d_64', 'design3d_64', 'disks2d_256', 'design3d_128', 'slab2d_512'])
 def test_fused_epilogue_matches_plain_schedule(name):
+    """The fused epilogue against the plain schedule, including the scalar 128- and 512-sample rows that the
+    autotuner times for the adjoint design problem and the batched slab."""
     wl = _cases()[name]()
     a, b = _solution(wl, True), _solution(wl, False)
     a.solve(None, rtol=0, maxiter=40)
