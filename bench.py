@@ -411,8 +411,9 @@ def run_secondary(args):
         source for all 256 sources, to 1e-5: single precision cannot reach 1e-8), each on the kernel variant the
         autotuner picks for it (chosen before the timed solves); and the uneven batch
         64 x 128^2 + 32 x 256^2 + 8 x 384^2 to 1e-8;
-      - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve in complex64 to 1e-6,
-        and in mixed precision to 1e-10, each gradient's error against the same gradient from FP64 solves.
+      - adjoint gradient (3D scalar design problem, 128^3, 32 sources): forward + adjoint solve in complex64 to 1e-6
+        (on the kernel variant the autotuner picks for a batch of the same problem), and in mixed precision to
+        1e-10, each gradient's error against the same gradient from FP64 solves.
     """
     import torch
     from macromax_b200 import Bound, Grid, Solution, adjoint, workloads
@@ -648,11 +649,19 @@ def run_secondary(args):
     k0 = 2 * np.pi / wl['wavelength']
     eps = torch.tensor(wl['epsilon'], dtype=torch.complex64, device='cuda', requires_grad=True)
     src = torch.tensor(wl['source'], dtype=torch.complex64, device='cuda')
+    # the pass-kernel variant of both solves: the autotuner's choice on a batch of the same problem, before timing
+    from macromax_b200 import autotune
+    from macromax_b200.batch import BatchSolution
+    tb = BatchSolution(grid, wl['source'], wl['epsilon'], bound=Bound(grid, thickness=wl['bound_thickness']),
+                       wavenumber=k0, dtype=np.complex64)
+    tuned_adj = autotune.tune(tb.engine, iters=10, use_cache=False)
+    tb.close()
+    del tb
     stats = {}
     torch.cuda.synchronize()
     a = time.perf_counter()
     E = adjoint.solve(eps, src, grid, k0, bound=Bound(grid, thickness=wl['bound_thickness']), rtol=1e-6,
-                      maxiter=100000, stats=stats)
+                      maxiter=100000, stats=stats, variant=tuned_adj['variant'])
     torch.cuda.synchronize()
     b = time.perf_counter()
     loss = -(E[:, 0][(slice(None),) + wl['patch']].abs() ** 2).sum()
@@ -670,7 +679,7 @@ def run_secondary(args):
         'voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / (c - a),
         'solve_s (forward + adjoint iterations only)': solve_s,
         'solve_voxel_iterations_per_s': 128 ** 3 * (int(fi.sum()) + int(ai.sum())) / solve_s,
-        'gradient_error_vs_fp64_adjoint': adjoint_fp64_error(wl, g32)}
+        'gradient_error_vs_fp64_adjoint': adjoint_fp64_error(wl, g32), 'kernel_variant': tuned_adj}
     del g32
     torch.cuda.empty_cache()
     # the same gradient with both solves in mixed precision (complex64 inner iterations, FP64 defect correction to

@@ -58,6 +58,9 @@ class _SolveFn(torch.autograd.Function):
             return _SolveFn._forward_mixed(ctx, epsilon, sources, problem, eps_np)
         bs = BatchSolution(grid, sources.detach(), eps_np, bound=problem.get('bound'), wavenumber=k0,
                            dtype=problem.get('dtype', np.complex64), device=sources.device)
+        if problem.get('variant') is not None:  # the pass-kernel variant for both solves (e.g. the autotuner's)
+            from . import autotune
+            autotune.set_variant(bs.engine, int(problem['variant']))
         t0 = _now()
         bs.solve(problem.get('rtol', 1e-6), problem.get('maxiter', 100000))
         problem.setdefault('stats', {})['forward_iterations'] = bs.iterations
@@ -160,17 +163,19 @@ class _SolveFn(torch.autograd.Function):
 
 def solve(epsilon: torch.Tensor, sources: torch.Tensor, grid: Grid, wavenumber: float, bound=None,
           dtype=np.complex64, rtol: float = 1e-6, maxiter: int = 100000, stats: dict | None = None,
-          precision: str = 'single') -> torch.Tensor:
+          precision: str = 'single', variant: int | None = None) -> torch.Tensor:
     """
     Differentiable solve: E [B, 1|3, *grid] for the isotropic permittivity ``epsilon`` [*grid] (real or complex)
     and sources [B, 1|3, *grid] (``source_distribution`` units).  Gradients flow to epsilon and sources through the
     adjoint solve above.  ``precision``: 'single' solves in ``dtype``; 'mixed' solves with complex64 inner iterations
-    and FP64 defect correction to ``rtol`` (the fields are complex128).
+    and FP64 defect correction to ``rtol`` (the fields are complex128).  ``variant``: the MMX_VARIANT_* pass-kernel
+    flags of the forward and adjoint solves in single precision (None: the plan's default), e.g. the choice of
+    ``autotune.tune`` on a batch of the same problem.
     """
     if precision not in ('single', 'mixed'):
         raise ValueError("precision must be 'single' or 'mixed'")
     problem = dict(grid=grid, wavenumber=float(wavenumber), bound=bound, dtype=dtype, rtol=rtol, maxiter=maxiter,
-                   precision=precision)
+                   precision=precision, variant=variant)
     if stats is not None:
         problem['stats'] = stats
     if sources.dim() == grid.ndim + 1:
